@@ -1,0 +1,437 @@
+#!/usr/bin/env python
+"""Benchmark of the VPM all-pairs hot path on B200.
+
+Metric: Biot-Savart Gpairs/s at N = 1M -- one fused self-induced velocity + velocity
+gradient (vortex stretching) evaluation of N = 2^20 particles in the FP32-compensated
+form, with the FP64 form and its relative error reported beside it.
+
+Workload: seeded random cloud (positions U[-1,1]^3, strengths N(0, 1e-3) per component,
+cores U(0.02, 0.05)), the throughput-sweep configuration at N = 2^20.  A step = one
+evaluation; pairs per step = N^2.  With --gpus P the targets are sharded over P ranks and
+the packed source records are all-gathered (NCCL) inside every step; `value` is the
+whole-job rate N^2 / (max over ranks of the step time).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "Biot-Savart Gpairs/s at N=1M: FP32-compensated vs FP64 at <=1e-6 rel err"
+UNIT = "Gpairs/s"
+# FP32-pipe work per pair of the fused velocity + stretching sweep:
+# 38 FP32 instructions = 20 FFMA + 12 FMUL + 6 FADD -> 58 flops (FMA = 2), 1 MUFU.RSQ.
+FLOPS_PER_PAIR_FUSED = 58
+FP32_OPS_PER_PAIR_FUSED = 38
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp32c_refined"])
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed", type=int, default=0)
+    return ap.parse_args()
+
+
+def workload(n, seed):
+    from openonda_b200 import configs
+
+    return configs.random_cloud(n, seed=seed)
+
+
+def workload_name(n, seed):
+    return (f"random cloud N={n} (x~U[-1,1]^3, alpha~N(0,1e-3), sigma~U(0.02,0.05), "
+            f"seed={seed}); one fused velocity + stretching evaluation")
+
+
+# ----------------------------------------------------------------------------------------
+# CPU baseline (the oracle's port of the reference's CPU module, all host threads)
+# ----------------------------------------------------------------------------------------
+def cpu_port_rate(field, seconds):
+    """Gpairs/s of velocity + stretching (CPU semantics) on a target subset x all sources."""
+    import oracle
+
+    x, a, s = field.positions, field.strengths, field.radii
+    n = len(x)
+    mod = oracle.cpu_fast
+    m = 16
+    t0 = time.perf_counter()
+    mod.selfinduced_velocity_range(x, a, s, 0, m)
+    mod.strength_gradients_range(x, a, s, 0, m)
+    dt = time.perf_counter() - t0
+    rate = m * n / max(dt, 1e-9)
+    m = int(max(16, min(n, rate * seconds / n)))
+    t0 = time.perf_counter()
+    mod.selfinduced_velocity_range(x, a, s, 0, m)
+    mod.strength_gradients_range(x, a, s, 0, m)
+    dt = time.perf_counter() - t0
+    return m * n / dt / 1e9, m, dt, oracle.num_threads()
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args):
+    """Reference arm: the reference's CPU path (oracle port, FP64, fast-math, all threads)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+
+    f = workload(args.n, args.seed)
+    x, a, s = f.positions, f.strengths, f.radii
+    n = len(x)
+    mod = oracle.cpu_fast
+    # size one step to ~6 s of CPU work so the whole run ends within a few minutes
+    m = 16
+    t0 = time.perf_counter()
+    mod.selfinduced_velocity_range(x, a, s, 0, m)
+    mod.strength_gradients_range(x, a, s, 0, m)
+    rate = m * n / max(time.perf_counter() - t0, 1e-9)
+    m = int(max(16, min(n, rate * 6.0 / n)))
+    times = []
+    for k in range(args.warmup + args.steps):
+        off = (k * m) % max(1, n - m)
+        t0 = time.perf_counter()
+        mod.selfinduced_velocity_range(x, a, s, off, off + m)
+        mod.strength_gradients_range(x, a, s, off, off + m)
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    t = float(np.mean(times))
+    value = m * n / t / 1e9
+    sample = (f"{m} targets x {n} sources per step (velocity + stretching, CPU semantics of "
+              f"ParticlesPhysics.py), {oracle.num_threads()} threads, {cpu_model()}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(args.n, args.seed), "n": args.n,
+                   "sample": sample},
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": oracle.num_threads(),
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------------------
+# clocks sampler
+# ----------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------------
+# B200 arm
+# ----------------------------------------------------------------------------------------
+def measure_fp32_peak(torch, kernels, dev):
+    props = torch.cuda.get_device_properties(dev)
+    blocks, threads, iters = props.multi_processor_count * 8, 256, 1 << 15
+    sink = torch.empty(blocks * threads, dtype=torch.float32, device=dev)
+    kernels.launch_fma_peak(False, blocks, threads, 64, sink)
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        kernels.launch_fma_peak(False, blocks, threads, iters, sink)
+        e1.record()
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        best = t if best is None else min(best, t)
+    fmas = blocks * threads * iters * 16
+    return 2.0 * fmas / best / 1e12
+
+
+def load_traffic():
+    path = os.path.join(HERE, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return None
+
+
+def normwise(got, ref):
+    d = (got - ref).abs().max()
+    r = ref.abs().max()
+    return float(d / r) if float(r) > 0 else float(d)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    from openonda_b200 import kernels
+    from openonda_b200.distributed import ShardedVelocityStretching, shard_range
+    from openonda_b200.vpm import ParticlesPhysicsB200 as pp
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    f = workload(args.n, args.seed)
+    n = f.n
+    start, stop = shard_range(n, rank, world)
+    # Inputs rounded to FP32 once, so that the FP64 run sees exactly the FP32 inputs.
+    x_h = f.positions.astype(np.float32).astype(np.float64)
+    a_h = f.strengths.astype(np.float32).astype(np.float64)
+    s_h = f.radii.astype(np.float32).astype(np.float64)
+    xs = torch.from_numpy(x_h[start:stop]).to(dev)
+    as_ = torch.from_numpy(a_h[start:stop]).to(dev)
+    ss = torch.from_numpy(s_h[start:stop]).to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def timed(op, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            op()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        evs = []
+        for _ in range(steps):
+            flush.fill_(1)  # L2 flush between timed steps, outside the events
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            e[0].record()
+            out = op()
+            e[1].record()
+            evs.append(e)
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        barrier()
+        t = sum(e[0].elapsed_time(e[1]) for e in evs) / 1e3
+        return max_over_ranks(t), out, clocks
+
+    # ---- FP32-compensated (headline) ----
+    sweep32 = ShardedVelocityStretching(n, precision=args.precision)
+    sweep_events = []
+
+    def step32():
+        sweep32.pack(xs, as_, ss)
+        rec = sweep32.exchange()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        e[0].record()
+        out = sweep32.sweep(rec)
+        e[1].record()
+        sweep_events.append(e)
+        return out
+
+    peak = measure_fp32_peak(torch, kernels, dev)
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    t32, (u32, g32), clocks = timed(step32, args.steps, args.warmup, sampler)
+    sweep_events = sweep_events[-args.steps:]
+    t_sweep = sum(e[0].elapsed_time(e[1]) for e in sweep_events) / 1e3 / args.steps
+    t_sweep = max_over_ranks(t_sweep)
+    u32, g32 = u32.clone(), g32.clone()
+    ms32 = t32 / args.steps * 1e3
+    value = float(n) * n / (t32 / args.steps) / 1e9
+
+    # ---- FP64 fused and FP64 drop-in (two separate sweeps, as the reference calls them) ----
+    sweep64 = ShardedVelocityStretching(n, precision="fp64")
+    t64, (u64, g64), _ = timed(lambda: sweep64(xs, as_, ss), args.fp64_steps, 1)
+    fp64_fused = float(n) * n / (t64 / args.fp64_steps) / 1e9
+    err_u = max_over_ranks(normwise(u32, u64))
+    err_g = max_over_ranks(normwise(g32, g64))
+    fp64_dropin = None
+    if world == 1:
+        xa = torch.from_numpy(x_h).to(dev)
+        aa = torch.from_numpy(a_h).to(dev)
+        sa = torch.from_numpy(s_h).to(dev)
+
+        def dropin():
+            return (kernels.selfinduced_velocity(xa, aa, sa, precision="fp64"),
+                    kernels.strength_gradients(xa, aa, sa, precision="fp64"))
+
+        tdi, _, _ = timed(dropin, 1, 1)
+        fp64_dropin = float(n) * n / tdi / 1e9
+        del xa, aa, sa
+
+    # ---- end to end through the public API, host buffers (pinned), copies timed ----
+    xp = torch.from_numpy(x_h[start:stop]).pin_memory()
+    ap_ = torch.from_numpy(a_h[start:stop]).pin_memory()
+    sp = torch.from_numpy(s_h[start:stop]).pin_memory()
+
+    def e2e_step():
+        if world == 1:
+            u, g = pp.get_selfinduced_velocity_and_strength_gradients(
+                xp, ap_, sp, precision=args.precision)
+        else:
+            u, g = sweep32(xp.to(dev, non_blocking=True), ap_.to(dev, non_blocking=True),
+                           sp.to(dev, non_blocking=True))
+            u, g = u.cpu(), g.cpu()
+        return u, g
+
+    for _ in range(1):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    barrier()
+    e2e_value = float(n) * n / (t_e2e / args.e2e_steps) / 1e9
+    m_local = stop - start
+    h2d = m_local * (3 + 3 + 1) * 8
+    d2h = m_local * 6 * 8
+
+    # ---- CPU baseline (rank 0, single GPU only) ----
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        rate, m, dt, cores = cpu_port_rate(f, args.cpu_seconds)
+        cpu = {"value": round(rate, 4), "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{m} targets x {n} sources, velocity + stretching (CPU semantics), "
+                         f"{dt:.1f} s, {cpu_model()}"}
+
+    if rank == 0:
+        pairs_per_launch = float(m_local) * n
+        achieved = FLOPS_PER_PAIR_FUSED * pairs_per_launch / t_sweep / 1e12
+        traffic = load_traffic()
+        tr = None
+        if traffic and traffic.get("kernel_traffic_bytes_per_pair") is not None:
+            tr = traffic["kernel_traffic_bytes_per_pair"] * pairs_per_launch
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms32, 3),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 pair terms + f64 carries", "data": "synthetic",
+            "config": {"workload": workload_name(n, args.seed), "n": n,
+                       "precision": args.precision,
+                       "parallelism": f"target shards x{world}, sources all-gathered",
+                       "l2": "flushed between timed steps (512 MiB write)"},
+            "fp64": {"fused_gpairs_s": round(fp64_fused, 3),
+                     "dropin_two_sweeps_gpairs_s":
+                         None if fp64_dropin is None else round(fp64_dropin, 3),
+                     "speedup_vs_fp64_fused": round(value / fp64_fused, 3),
+                     "speedup_vs_fp64_dropin":
+                         None if fp64_dropin is None else round(value / fp64_dropin, 3)},
+            "rel_err_vs_fp64": {"velocity": err_u, "stretching": err_g},
+            "roofline": {"bound": "fp32", "achieved": round(achieved, 3),
+                         "peak": round(peak, 3), "unit": "TFLOP/s",
+                         "frac": round(achieved / peak, 4), "traffic": tr,
+                         "peak_source": "FFMA microbenchmark measured in this run",
+                         "flops_per_pair": FLOPS_PER_PAIR_FUSED,
+                         "fp32_pipe_frac": round(achieved / peak * 2 * FP32_OPS_PER_PAIR_FUSED
+                                                 / FLOPS_PER_PAIR_FUSED, 4)},
+            "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "cpu_baseline": cpu,
+            "gpu_launches": args.steps * sweep32.kernel_launches_per_call,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,160 @@
+/*
+ * vpm_b200.h -- C ABI of the B200 (sm_100a) VPM pair-sum library (libvpm_b200.so).
+ *
+ * Every compute entry point replaces one module-level function of OpenONDA's Numba-CUDA
+ * physics module, OpenONDA/solvers/VPM/ParticlesPhysicsCuda.py, which
+ * vpmModule.ParticleSystem selects in _load_physics_module (vpmModule.py:141-154).
+ *
+ * Conventions
+ *   - Arrays are DEVICE pointers in the reference's layout: positions, strengths and
+ *     outputs (n,3) row-major float64; radii and viscosities (n,) float64.
+ *   - `precision`: VPM_FP64 computes in FP64 and is the exact drop-in (matches the
+ *     reference's routine to 1e-12 relative); VPM_FP32C computes the pair terms in FP32
+ *     with FP64 carries (inputs are rounded to FP32 once, outputs are FP64);
+ *     VPM_FP32C_REFINED adds one Newton step to the hardware rsqrt.
+ *   - `workspace`/`workspace_bytes`: caller-owned device scratch of at least
+ *     vpm_workspace_bytes(op, precision, m, n) bytes, 256-byte aligned.  The library never
+ *     allocates.
+ *   - `stream`: a cudaStream_t (NULL = legacy default stream).  Calls are asynchronous
+ *     with respect to the host; scalar results are written to a device double.
+ *   - Return value: VPM_OK (0) or an error code; vpm_last_error() gives the message for
+ *     the calling thread.  Inputs are never modified; nothing throws across the ABI.
+ *   - Radii must be positive.  Results are deterministic for a given device and sizes.
+ */
+#ifndef VPM_B200_H
+#define VPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VPM_ABI_VERSION 1
+
+enum vpm_status {
+  VPM_OK = 0,
+  VPM_ERR_ARG = 1,        /* bad size, null pointer, unknown op or precision */
+  VPM_ERR_ALIGN = 2,      /* workspace not 256-byte aligned */
+  VPM_ERR_WORKSPACE = 3,  /* workspace smaller than vpm_workspace_bytes() */
+  VPM_ERR_CUDA = 4,       /* CUDA runtime error (launch, attribute query) */
+  VPM_ERR_ARCH = 5        /* current device is not compute capability 10.0 */
+};
+
+enum vpm_precision { VPM_FP64 = 0, VPM_FP32C = 1, VPM_FP32C_REFINED = 2 };
+
+enum vpm_op {
+  VPM_OP_SELFINDUCED_VELOCITY = 0,
+  VPM_OP_INDUCED_VELOCITY_AT = 1,
+  VPM_OP_VORTICITY_FIELD_AT = 2,
+  VPM_OP_STRENGTH_GRADIENTS = 3,
+  VPM_OP_STRENGTH_GRADIENTS_PSE = 4,
+  VPM_OP_TOTAL_KINETIC_ENERGY = 5,
+  VPM_OP_TOTAL_HELICITY = 6,
+  VPM_OP_TOTAL_ENSTROPHY = 7,
+  VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS = 8
+};
+
+/* ---- library information ------------------------------------------------------------ */
+int vpm_abi_version(void);
+const char* vpm_last_error(void);
+/* Check that the current device is sm_100 (B200); VPM_ERR_ARCH otherwise. */
+int vpm_check_device(void);
+/* Read (and optionally clear) the device error word: bit 0 = a bounded wait timed out. */
+int vpm_device_errors(int* out, int clear);
+/* Scratch bytes `op` needs for m targets and n sources (m = n for self sums). */
+size_t vpm_workspace_bytes(int op, int precision, int64_t m, int64_t n);
+/* Launch plan of `op`: target blocks, source splits, threads/block, targets/thread. */
+int vpm_plan_info(int op, int precision, int64_t m, int64_t n, int64_t* target_blocks,
+                  int* splits, int* threads, int* targets_per_thread);
+
+/* ---- reference entry points ------------------------------------------------------------ */
+
+/* get_induced_velocity_at (ParticlesPhysicsCuda.py:11-34, kernel :39-97):
+ * velocity at m probe points from n particles, source core sigma_j, pairs r^2<=1e-8 skipped. */
+int vpm_induced_velocity_at(const double* targets, int64_t m, const double* positions,
+                            const double* strengths, const double* radii, int64_t n,
+                            double* velocities, int precision, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
+/* get_selfinduced_velocity (ParticlesPhysicsCuda.py:103-127, kernel :133-191):
+ * j != i, pair core (sigma_i + sigma_j)/2. */
+int vpm_selfinduced_velocity(const double* positions, const double* strengths,
+                             const double* radii, int64_t n, double* velocities, int precision,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* get_vorticity_field_at (ParticlesPhysicsCuda.py:198-219, kernel :291-346): zeta-kernel
+ * vorticity at m probe points.  One output row per target (the reference sizes its output by
+ * n and is only correct for m == n; for m == n the results agree). */
+int vpm_vorticity_field_at(const double* targets, int64_t m, const double* positions,
+                           const double* strengths, const double* radii, int64_t n,
+                           double* vorticities, int precision, void* workspace,
+                           size_t workspace_bytes, void* stream);
+
+/* get_strength_gradients (ParticlesPhysicsCuda.py:351-370, kernel :375-445): vortex
+ * stretching, transpose scheme. */
+int vpm_strength_gradients(const double* positions, const double* strengths,
+                           const double* radii, int64_t n, double* dalpha_dt, int precision,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
+/* get_strength_gradients_PSE (ParticlesPhysicsCuda.py:452-473, kernel :478-530):
+ * PSE diffusion with the target's viscosity nu_i. */
+int vpm_strength_gradients_pse(const double* positions, const double* strengths,
+                               const double* radii, const double* viscosities, int64_t n,
+                               double* dalpha_dt, int precision, void* workspace,
+                               size_t workspace_bytes, void* stream);
+
+/* get_total_kinetic_energy (ParticlesPhysicsCuda.py:537-558, kernel :563-642).
+ * The accumulator starts at zero (the reference never clears it). */
+int vpm_total_kinetic_energy(const double* positions, const double* strengths,
+                             const double* radii, int64_t n, double* energy, int precision,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* get_total_helicity (ParticlesPhysicsCuda.py:647-668, kernel :673-750).
+ * ref_extra_4pi != 0 keeps the wrapper's second division by 4*pi (:668). */
+int vpm_total_helicity(const double* positions, const double* strengths, const double* radii,
+                       int64_t n, int ref_extra_4pi, double* helicity, int precision,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
+/* get_total_enstrophy (ParticlesPhysicsCuda.py:756-777, kernel :867-920), all pairs.
+ * ref_extra_4pi != 0 keeps the wrapper's second division by 4*pi (:777). */
+int vpm_total_enstrophy(const double* positions, const double* strengths, const double* radii,
+                        int64_t n, int ref_extra_4pi, double* enstrophy, int precision,
+                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* get_selfinduced_velocity + get_strength_gradients (vpmModule.py:704 and :753-774 call
+ * them on the same positions/strengths/radii) fused into one sweep. */
+int vpm_velocity_and_strength_gradients(const double* positions, const double* strengths,
+                                        const double* radii, int64_t n, double* velocities,
+                                        double* dalpha_dt, int precision, void* workspace,
+                                        size_t workspace_bytes, void* stream);
+
+/* ---- pre-packed records (device-resident state, target shards) ----------------------- */
+/* Bytes of one packed particle record: 32 (FP32 forms) or 64 (VPM_FP64). */
+size_t vpm_record_bytes(int precision);
+/* Pack n particles from the reference layout into records {x,y,z,sigma,ax,ay,az,nu} of the
+ * compute precision (viscosities may be NULL: nu = 0).  `records` is 16-byte aligned. */
+int vpm_pack_records(const double* positions, const double* strengths, const double* radii,
+                     const double* viscosities, int64_t n, int precision, void* records,
+                     void* stream);
+/* Self sum `op` (any VPM_OP_* except the two probes) for the m targets
+ * records[target_begin, target_begin + m) against all n source records; outputs hold m
+ * rows (out2 is the stretching output of VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS, scalars
+ * are partial sums over the m targets).  This is the unit of work one rank runs when the
+ * targets are sharded across GPUs.  Same workspace rule as the reference entry points. */
+int vpm_sweep_records(int op, const void* records, int64_t n, int64_t target_begin, int64_t m,
+                      int ref_extra_4pi, double* out, double* out2, int precision,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- measurement helpers -------------------------------------------------------------- */
+/* FP32 FMA (fp64 != 0: FP64 FMA) throughput kernel: blocks x threads threads each run
+ * `iters` iterations of 16 independent FMA chains; one value per thread lands in `sink`
+ * (blocks*threads floats or doubles).  FMA count = blocks*threads*iters*16. */
+int vpm_launch_fma_peak(int fp64, int blocks, int threads, int iters, void* sink, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VPM_B200_H */

@@ -1,0 +1,754 @@
+// vpm_abi.cu -- C-ABI entry points, launch planning, pack and finalize kernels.
+//
+// One call = pack (reference AoS float64 -> packed records in the compute precision,
+// inside the caller's workspace) -> tiled sweep (partials per source split, FP64) ->
+// finalize (sum the splits in order, apply target-only factors, write the reference's
+// output layout).  Scalars reduce the per-target values in a single block in a fixed
+// order, so every result is deterministic.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <utility>
+
+#include "vpm_b200.h"
+#include "vpm_sweep.cuh"
+
+namespace vpm {
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  return fail(VPM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+constexpr size_t kAlign = 256;
+size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+// ---- kernel configurations -----------------------------------------------------------
+template <class T>
+struct Cfg;
+template <>
+struct Cfg<float> {
+  static constexpr int R = 4, THREADS = 128, TILE = 256, STAGES = 2;
+};
+template <>
+struct Cfg<double> {
+  static constexpr int R = 2, THREADS = 128, TILE = 128, STAGES = 2;
+};
+
+constexpr int kMaxSplits = 64;
+constexpr int64_t kMinChunk = 256;
+constexpr size_t kMaxPartialBytes = size_t(4) << 30;
+
+struct Plan {
+  int64_t tblocks = 0;
+  int splits = 1;
+  int64_t chunk = 0;
+  size_t smem = 0;
+  int threads = 0;
+  int r = 0;
+  int nv = 0;
+};
+
+struct DevInfo {
+  int sms = 0;
+  int major = 0, minor = 0;
+};
+
+std::mutex g_mu;
+std::unordered_map<int, DevInfo> g_dev;
+std::map<std::pair<const void*, int>, int> g_occ;  // (kernel, device) -> resident blocks/SM
+
+int device_info(DevInfo* out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_dev.find(dev);
+  if (it == g_dev.end()) {
+    DevInfo d;
+    e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
+    cudaDeviceGetAttribute(&d.major, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&d.minor, cudaDevAttrComputeCapabilityMinor, dev);
+    it = g_dev.emplace(dev, d).first;
+  }
+  *out = it->second;
+  return VPM_OK;
+}
+
+int check_arch() {
+  DevInfo d;
+  int rc = device_info(&d);
+  if (rc) return rc;
+  if (d.major != 10 || d.minor != 0)
+    return fail(VPM_ERR_ARCH, "libvpm_b200 is built for sm_100a (B200); current device is sm_" +
+                                  std::to_string(d.major) + std::to_string(d.minor));
+  return VPM_OK;
+}
+
+template <class Op, class T>
+struct Sweep {
+  using C = Cfg<T>;
+  static constexpr int NV = Op::NV;
+  static constexpr size_t kSmem = size_t(C::STAGES) * C::TILE * sizeof(Rec<T>);
+  static void* kernel() {
+    return reinterpret_cast<void*>(&sweep_kernel<Op, T, C::R, C::THREADS, C::TILE, C::STAGES>);
+  }
+
+  static int plan(int64_t m, int64_t n, Plan* p) {
+    DevInfo d;
+    int rc = device_info(&d);
+    if (rc) return rc;
+    int occ = 0;
+    {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      const auto key = std::make_pair(static_cast<const void*>(kernel()), dev);
+      std::lock_guard<std::mutex> lk(g_mu);
+      auto it = g_occ.find(key);
+      if (it != g_occ.end()) {
+        occ = it->second;
+      } else {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel(),
+                                                                      C::THREADS, kSmem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        g_occ[key] = occ;
+      }
+    }
+    if (occ < 1) occ = 1;
+    const int64_t per_block = int64_t(C::THREADS) * C::R;
+    p->tblocks = (m + per_block - 1) / per_block;
+    p->smem = kSmem;
+    p->threads = C::THREADS;
+    p->r = C::R;
+    p->nv = NV;
+    p->splits = 1;
+    p->chunk = n;
+    if (n <= 0 || m <= 0) return VPM_OK;
+    const double slots = double(d.sms) * occ;
+    double best = -1.0;
+    for (int s = 1; s <= kMaxSplits; ++s) {
+      int64_t chunk = (n + s - 1) / s;
+      chunk = (chunk + kCarryWindow - 1) / kCarryWindow * kCarryWindow;
+      if (s > 1 && chunk < kMinChunk) break;
+      const int64_t se = (n + chunk - 1) / chunk;
+      if (se != s) continue;
+      if (size_t(se) * NV * size_t(m) * sizeof(double) > kMaxPartialBytes) break;
+      const double waves = double(p->tblocks) * se / slots;
+      const double eff = waves / std::ceil(waves);
+      const double score = eff * (1.0 - 0.003 * (se - 1));
+      if (score > best + 1e-12) {
+        best = score;
+        p->splits = int(se);
+        p->chunk = chunk;
+      }
+    }
+    return VPM_OK;
+  }
+
+  static size_t partial_bytes(const Plan& p, int64_t m) {
+    return size_t(p.splits) * NV * size_t(m) * sizeof(double);
+  }
+
+  static int launch(const Plan& p, const Rec<T>* tgt, int64_t m, int64_t tgt_offset,
+                    const Rec<T>* src, int64_t n, double* partial, cudaStream_t st) {
+    SweepArgs<T> a{tgt, m, tgt_offset, src, n, p.chunk, partial};
+    dim3 grid(unsigned(p.tblocks), unsigned(p.splits));
+    sweep_kernel<Op, T, C::R, C::THREADS, C::TILE, C::STAGES><<<grid, C::THREADS, p.smem, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
+    return VPM_OK;
+  }
+};
+
+// ---- pack kernels ----------------------------------------------------------------------
+template <class T>
+__global__ void pack_particles_kernel(const double* __restrict__ pos,
+                                      const double* __restrict__ str,
+                                      const double* __restrict__ rad,
+                                      const double* __restrict__ nu, int64_t n,
+                                      Rec<T>* __restrict__ out) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Rec<T> r;
+  r.x = T(pos[3 * i]);
+  r.y = T(pos[3 * i + 1]);
+  r.z = T(pos[3 * i + 2]);
+  r.s = rad ? T(rad[i]) : T(0);
+  r.ax = str ? T(str[3 * i]) : T(0);
+  r.ay = str ? T(str[3 * i + 1]) : T(0);
+  r.az = str ? T(str[3 * i + 2]) : T(0);
+  r.nu = nu ? T(nu[i]) : T(0);
+  out[i] = r;
+}
+
+template <class T>
+int pack(const double* pos, const double* str, const double* rad, const double* nu, int64_t n,
+         Rec<T>* out, cudaStream_t st) {
+  if (n <= 0) return VPM_OK;
+  const int threads = 256;
+  const int64_t blocks = (n + threads - 1) / threads;
+  pack_particles_kernel<T><<<unsigned(blocks), threads, 0, st>>>(pos, str, rad, nu, n, out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "pack launch");
+  return VPM_OK;
+}
+
+// ---- finalize kernels -----------------------------------------------------------------
+enum FinKind { FIN_VEL = 0, FIN_VORT = 1, FIN_STRETCH = 2, FIN_PSE = 3, FIN_VELSTRETCH = 4 };
+
+template <int NV>
+__device__ __forceinline__ void sum_splits(const double* __restrict__ part, int splits, int64_t m,
+                                           int64_t i, double (&v)[NV]) {
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = 0.0;
+  for (int s = 0; s < splits; ++s) {
+    const double* p = part + int64_t(s) * NV * m;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] += p[int64_t(k) * m + i];
+  }
+}
+
+template <class T, int KIND, int NV>
+__global__ void finalize_vec_kernel(const double* __restrict__ part, int splits, int64_t m,
+                                    const Rec<T>* __restrict__ tgt, double* __restrict__ out,
+                                    double* __restrict__ out2) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double v[NV];
+  sum_splits<NV>(part, splits, m, i, v);
+  if constexpr (KIND == FIN_VEL) {
+    out[3 * i] = -v[0] * kOneOver4Pi;
+    out[3 * i + 1] = -v[1] * kOneOver4Pi;
+    out[3 * i + 2] = -v[2] * kOneOver4Pi;
+  } else if constexpr (KIND == FIN_VORT) {
+    const double c = 7.5 * kOneOver4Pi;
+    out[3 * i] = v[0] * c;
+    out[3 * i + 1] = v[1] * c;
+    out[3 * i + 2] = v[2] * c;
+  } else if constexpr (KIND == FIN_PSE) {
+    const double c = 105.0 * double(tgt[i].nu) * kOneOver4Pi;
+    out[3 * i] = v[0] * c;
+    out[3 * i + 1] = v[1] * c;
+    out[3 * i + 2] = v[2] * c;
+  } else {
+    constexpr int o = (KIND == FIN_VELSTRETCH) ? 3 : 0;
+    double* so = (KIND == FIN_VELSTRETCH) ? out2 : out;
+    if constexpr (KIND == FIN_VELSTRETCH) {
+      out[3 * i] = -v[0] * kOneOver4Pi;
+      out[3 * i + 1] = -v[1] * kOneOver4Pi;
+      out[3 * i + 2] = -v[2] * kOneOver4Pi;
+    }
+    const double bx = double(tgt[i].ax), by = double(tgt[i].ay), bz = double(tgt[i].az);
+    const double Ax = v[o], Ay = v[o + 1], Az = v[o + 2];
+    so[3 * i] = (by * Az - bz * Ay + 3.0 * v[o + 3]) * kOneOver4Pi;
+    so[3 * i + 1] = (bz * Ax - bx * Az + 3.0 * v[o + 4]) * kOneOver4Pi;
+    so[3 * i + 2] = (bx * Ay - by * Ax + 3.0 * v[o + 5]) * kOneOver4Pi;
+  }
+}
+
+constexpr int kReduceThreads = 1024;
+
+// Single-block, fixed-order reduction of  sign * a_i . V_i  over all targets.
+template <class T>
+__global__ void __launch_bounds__(kReduceThreads)
+finalize_dot_kernel(const double* __restrict__ part, int splits, int64_t m,
+                    const Rec<T>* __restrict__ tgt, double scale, double* __restrict__ out) {
+  __shared__ double red[kReduceThreads];
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < m; i += kReduceThreads) {
+    double v[3];
+    sum_splits<3>(part, splits, m, i, v);
+    acc += double(tgt[i].ax) * v[0] + double(tgt[i].ay) * v[1] + double(tgt[i].az) * v[2];
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = kReduceThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = red[0] * scale;
+}
+
+__global__ void write_scalar_kernel(double* out, double v) { out[0] = v; }
+
+template <class T, int KIND, int NV>
+int finalize_vec(const double* part, int splits, int64_t m, const Rec<T>* tgt, double* out,
+                 double* out2, cudaStream_t st) {
+  if (m <= 0) return VPM_OK;
+  const int threads = 256;
+  finalize_vec_kernel<T, KIND, NV>
+      <<<unsigned((m + threads - 1) / threads), threads, 0, st>>>(part, splits, m, tgt, out, out2);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "finalize launch");
+  return VPM_OK;
+}
+
+__global__ void zero_kernel(double* p, int64_t count) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < count) p[i] = 0.0;
+}
+
+int zero_out(double* p, int64_t count, cudaStream_t st) {
+  if (count <= 0) return VPM_OK;
+  zero_kernel<<<unsigned((count + 255) / 256), 256, 0, st>>>(p, count);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "zero launch");
+  return VPM_OK;
+}
+
+// ---- operator selection -----------------------------------------------------------------
+template <class T, bool REFINE>
+struct Ops {
+  using Vel = OpVel<T, REFINE>;
+  using VelAt = OpVelAt<T, REFINE>;
+  using VortAt = OpVortAt<T, REFINE>;
+  using Stretch = OpStretch<T, REFINE>;
+  using Pse = OpPse<T, REFINE>;
+  using Ke = OpKe<T, REFINE>;
+  using Ens = OpEns<T, REFINE>;
+  using VelStretch = OpVelStretch<T, REFINE>;
+};
+
+bool is_probe(int op) { return op == VPM_OP_INDUCED_VELOCITY_AT || op == VPM_OP_VORTICITY_FIELD_AT; }
+
+template <class T, bool REFINE>
+int plan_op(int op, int64_t m, int64_t n, Plan* p) {
+  using O = Ops<T, REFINE>;
+  switch (op) {
+    case VPM_OP_SELFINDUCED_VELOCITY:
+    case VPM_OP_TOTAL_HELICITY:
+      return Sweep<typename O::Vel, T>::plan(m, n, p);
+    case VPM_OP_INDUCED_VELOCITY_AT:
+      return Sweep<typename O::VelAt, T>::plan(m, n, p);
+    case VPM_OP_VORTICITY_FIELD_AT:
+      return Sweep<typename O::VortAt, T>::plan(m, n, p);
+    case VPM_OP_STRENGTH_GRADIENTS:
+      return Sweep<typename O::Stretch, T>::plan(m, n, p);
+    case VPM_OP_STRENGTH_GRADIENTS_PSE:
+      return Sweep<typename O::Pse, T>::plan(m, n, p);
+    case VPM_OP_TOTAL_KINETIC_ENERGY:
+      return Sweep<typename O::Ke, T>::plan(m, n, p);
+    case VPM_OP_TOTAL_ENSTROPHY:
+      return Sweep<typename O::Ens, T>::plan(m, n, p);
+    case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
+      return Sweep<typename O::VelStretch, T>::plan(m, n, p);
+    default:
+      return fail(VPM_ERR_ARG, "unknown op " + std::to_string(op));
+  }
+}
+
+struct Layout {
+  size_t src_off = 0, tgt_off = 0, part_off = 0, total = 0;
+};
+
+template <class T>
+Layout layout_for(int op, const Plan& p, int64_t m, int64_t n) {
+  Layout L;
+  L.src_off = 0;
+  size_t off = align_up(size_t(n > 0 ? n : 0) * sizeof(Rec<T>));
+  L.tgt_off = off;
+  if (is_probe(op)) off = align_up(off + size_t(m > 0 ? m : 0) * sizeof(Rec<T>));
+  L.part_off = off;
+  off = align_up(off + size_t(p.splits) * p.nv * size_t(m > 0 ? m : 0) * sizeof(double));
+  L.total = off;
+  return L;
+}
+
+template <class T, bool REFINE>
+int workspace_for(int op, int64_t m, int64_t n, Layout* L, Plan* p) {
+  int rc = plan_op<T, REFINE>(op, m, n, p);
+  if (rc) return rc;
+  *L = layout_for<T>(op, *p, m, n);
+  return VPM_OK;
+}
+
+struct Call {
+  int op;
+  const double* tgt;  // probe targets (m,3) or null for self sums
+  int64_t m;
+  const double* pos;
+  const double* str;
+  const double* rad;
+  const double* nu;
+  int64_t n;
+  double* out;
+  double* out2;
+  int ref_extra_4pi;
+  void* ws;
+  size_t ws_bytes;
+  cudaStream_t st;
+  const void* records = nullptr;  // pre-packed sources (self sums); null = pack from AoS
+  int64_t tgt_begin = 0;          // self sums: targets are records[tgt_begin, tgt_begin + m)
+};
+
+template <class T, bool REFINE>
+int run(const Call& c) {
+  using O = Ops<T, REFINE>;
+  int rc = check_arch();
+  if (rc) return rc;
+  const bool scalar = c.op == VPM_OP_TOTAL_KINETIC_ENERGY || c.op == VPM_OP_TOTAL_HELICITY ||
+                      c.op == VPM_OP_TOTAL_ENSTROPHY;
+  // Empty inputs: zero outputs, no sweep, no workspace needed.
+  if (c.m <= 0 || c.n <= 0) {
+    if (scalar) {
+      write_scalar_kernel<<<1, 1, 0, c.st>>>(c.out, 0.0);
+      cudaError_t e = cudaGetLastError();
+      return e == cudaSuccess ? VPM_OK : cuda_fail(e, "write launch");
+    }
+    rc = zero_out(c.out, 3 * (c.m > 0 ? c.m : 0), c.st);
+    if (!rc && c.out2) rc = zero_out(c.out2, 3 * (c.m > 0 ? c.m : 0), c.st);
+    return rc;
+  }
+
+  Plan p;
+  Layout L;
+  rc = workspace_for<T, REFINE>(c.op, c.m, c.n, &L, &p);
+  if (rc) return rc;
+  if (c.ws == nullptr) return fail(VPM_ERR_WORKSPACE, "workspace is null");
+  if (reinterpret_cast<uintptr_t>(c.ws) % kAlign != 0)
+    return fail(VPM_ERR_ALIGN, "workspace must be 256-byte aligned");
+  if (c.ws_bytes < L.total)
+    return fail(VPM_ERR_WORKSPACE, "workspace has " + std::to_string(c.ws_bytes) +
+                                       " bytes, needs " + std::to_string(L.total));
+  char* ws = static_cast<char*>(c.ws);
+  Rec<T>* src = c.records ? const_cast<Rec<T>*>(static_cast<const Rec<T>*>(c.records))
+                          : reinterpret_cast<Rec<T>*>(ws + L.src_off);
+  Rec<T>* tgt = is_probe(c.op) ? reinterpret_cast<Rec<T>*>(ws + L.tgt_off) : src + c.tgt_begin;
+  double* part = reinterpret_cast<double*>(ws + L.part_off);
+
+  if (!c.records) {
+    rc = pack<T>(c.pos, c.str, c.rad, c.nu, c.n, src, c.st);
+    if (rc) return rc;
+  }
+  if (is_probe(c.op)) {
+    rc = pack<T>(c.tgt, nullptr, nullptr, nullptr, c.m, tgt, c.st);
+    if (rc) return rc;
+  }
+
+  switch (c.op) {
+    case VPM_OP_SELFINDUCED_VELOCITY:
+      rc = Sweep<typename O::Vel, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+      if (!rc) rc = finalize_vec<T, FIN_VEL, 3>(part, p.splits, c.m, tgt, c.out, nullptr, c.st);
+      return rc;
+    case VPM_OP_INDUCED_VELOCITY_AT:
+      rc = Sweep<typename O::VelAt, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+      if (!rc) rc = finalize_vec<T, FIN_VEL, 3>(part, p.splits, c.m, tgt, c.out, nullptr, c.st);
+      return rc;
+    case VPM_OP_VORTICITY_FIELD_AT:
+      rc = Sweep<typename O::VortAt, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+      if (!rc) rc = finalize_vec<T, FIN_VORT, 3>(part, p.splits, c.m, tgt, c.out, nullptr, c.st);
+      return rc;
+    case VPM_OP_STRENGTH_GRADIENTS:
+      rc = Sweep<typename O::Stretch, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+      if (!rc)
+        rc = finalize_vec<T, FIN_STRETCH, 6>(part, p.splits, c.m, tgt, c.out, nullptr, c.st);
+      return rc;
+    case VPM_OP_STRENGTH_GRADIENTS_PSE:
+      rc = Sweep<typename O::Pse, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+      if (!rc) rc = finalize_vec<T, FIN_PSE, 3>(part, p.splits, c.m, tgt, c.out, nullptr, c.st);
+      return rc;
+    case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
+      rc = Sweep<typename O::VelStretch, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+      if (!rc)
+        rc = finalize_vec<T, FIN_VELSTRETCH, 9>(part, p.splits, c.m, tgt, c.out, c.out2, c.st);
+      return rc;
+    case VPM_OP_TOTAL_KINETIC_ENERGY:
+    case VPM_OP_TOTAL_HELICITY:
+    case VPM_OP_TOTAL_ENSTROPHY: {
+      double scale = 0.0;
+      if (c.op == VPM_OP_TOTAL_KINETIC_ENERGY) {
+        rc = Sweep<typename O::Ke, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+        scale = 1.0 / (16.0 * kPi);
+      } else if (c.op == VPM_OP_TOTAL_HELICITY) {
+        rc = Sweep<typename O::Vel, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+        scale = -1.0 / (4.0 * kPi);
+        if (c.ref_extra_4pi) scale /= 4.0 * kPi;
+      } else {
+        rc = Sweep<typename O::Ens, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+        scale = 1.0 / (8.0 * kPi);
+        if (c.ref_extra_4pi) scale /= 4.0 * kPi;
+      }
+      if (rc) return rc;
+      finalize_dot_kernel<T><<<1, kReduceThreads, 0, c.st>>>(part, p.splits, c.m, tgt, scale,
+                                                             c.out);
+      cudaError_t e = cudaGetLastError();
+      return e == cudaSuccess ? VPM_OK : cuda_fail(e, "reduce launch");
+    }
+    default:
+      return fail(VPM_ERR_ARG, "unknown op " + std::to_string(c.op));
+  }
+}
+
+int dispatch(const Call& c, int precision) {
+  if (c.n < 0 || c.m < 0) return fail(VPM_ERR_ARG, "negative size");
+  if (c.records) {
+    if (is_probe(c.op)) return fail(VPM_ERR_ARG, "record entry points are for self sums");
+    if (c.tgt_begin < 0 || c.tgt_begin + c.m > c.n)
+      return fail(VPM_ERR_ARG, "target range outside the records");
+    if (reinterpret_cast<uintptr_t>(c.records) % 16 != 0)
+      return fail(VPM_ERR_ALIGN, "records must be 16-byte aligned");
+  } else {
+    if (c.n > 0 && (!c.pos || !c.rad)) return fail(VPM_ERR_ARG, "null input pointer");
+    if (c.n > 0 && !c.str) return fail(VPM_ERR_ARG, "null strengths pointer");
+  }
+  if (c.m > 0 && !c.out) return fail(VPM_ERR_ARG, "null output pointer");
+  if (is_probe(c.op) && c.m > 0 && !c.tgt) return fail(VPM_ERR_ARG, "null targets pointer");
+  if (c.op == VPM_OP_STRENGTH_GRADIENTS_PSE && c.n > 0 && !c.nu && !c.records)
+    return fail(VPM_ERR_ARG, "null viscosities pointer");
+  if (c.op == VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS && c.m > 0 && !c.out2)
+    return fail(VPM_ERR_ARG, "null second output pointer");
+  switch (precision) {
+    case VPM_FP64:
+      return run<double, false>(c);
+    case VPM_FP32C:
+      return run<float, false>(c);
+    case VPM_FP32C_REFINED:
+      return run<float, true>(c);
+    default:
+      return fail(VPM_ERR_ARG, "unknown precision " + std::to_string(precision));
+  }
+}
+
+// ---- FMA throughput kernels ------------------------------------------------------------
+template <class T>
+__global__ void fma_peak_kernel(int iters, T* sink) {
+  T a[16];
+  const T m = T(1.0) - T(1e-7) * T(threadIdx.x & 7);
+  const T b = T(1e-9) * T(blockIdx.x & 3);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) a[k] = T(threadIdx.x + k);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) a[k] = fma(a[k], m, b);
+  }
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) s += a[k];
+  sink[int64_t(blockIdx.x) * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace
+}  // namespace vpm
+
+using namespace vpm;
+
+extern "C" {
+
+int vpm_abi_version(void) { return VPM_ABI_VERSION; }
+
+const char* vpm_last_error(void) { return g_last_error.c_str(); }
+
+int vpm_check_device(void) { return check_arch(); }
+
+int vpm_device_errors(int* out, int clear) {
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, g_device_errors, sizeof(int));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyFromSymbol");
+  if (out) *out = v;
+  if (clear) {
+    const int z = 0;
+    e = cudaMemcpyToSymbol(g_device_errors, &z, sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyToSymbol");
+  }
+  return VPM_OK;
+}
+
+size_t vpm_workspace_bytes(int op, int precision, int64_t m, int64_t n) {
+  Plan p;
+  Layout L;
+  int rc;
+  switch (precision) {
+    case VPM_FP64:
+      rc = workspace_for<double, false>(op, m, n, &L, &p);
+      break;
+    case VPM_FP32C:
+      rc = workspace_for<float, false>(op, m, n, &L, &p);
+      break;
+    case VPM_FP32C_REFINED:
+      rc = workspace_for<float, true>(op, m, n, &L, &p);
+      break;
+    default:
+      fail(VPM_ERR_ARG, "unknown precision");
+      return 0;
+  }
+  return rc ? 0 : L.total;
+}
+
+int vpm_plan_info(int op, int precision, int64_t m, int64_t n, int64_t* target_blocks,
+                  int* splits, int* threads, int* targets_per_thread) {
+  Plan p;
+  int rc;
+  switch (precision) {
+    case VPM_FP64:
+      rc = plan_op<double, false>(op, m, n, &p);
+      break;
+    case VPM_FP32C:
+      rc = plan_op<float, false>(op, m, n, &p);
+      break;
+    case VPM_FP32C_REFINED:
+      rc = plan_op<float, true>(op, m, n, &p);
+      break;
+    default:
+      return fail(VPM_ERR_ARG, "unknown precision");
+  }
+  if (rc) return rc;
+  if (target_blocks) *target_blocks = p.tblocks;
+  if (splits) *splits = p.splits;
+  if (threads) *threads = p.threads;
+  if (targets_per_thread) *targets_per_thread = p.r;
+  return VPM_OK;
+}
+
+int vpm_induced_velocity_at(const double* targets, int64_t m, const double* positions,
+                            const double* strengths, const double* radii, int64_t n,
+                            double* velocities, int precision, void* workspace,
+                            size_t workspace_bytes, void* stream) {
+  Call c{VPM_OP_INDUCED_VELOCITY_AT, targets, m, positions, strengths, radii, nullptr, n,
+         velocities, nullptr, 0, workspace, workspace_bytes, static_cast<cudaStream_t>(stream)};
+  return dispatch(c, precision);
+}
+
+int vpm_selfinduced_velocity(const double* positions, const double* strengths,
+                             const double* radii, int64_t n, double* velocities, int precision,
+                             void* workspace, size_t workspace_bytes, void* stream) {
+  Call c{VPM_OP_SELFINDUCED_VELOCITY, nullptr, n, positions, strengths, radii, nullptr, n,
+         velocities, nullptr, 0, workspace, workspace_bytes, static_cast<cudaStream_t>(stream)};
+  return dispatch(c, precision);
+}
+
+int vpm_vorticity_field_at(const double* targets, int64_t m, const double* positions,
+                           const double* strengths, const double* radii, int64_t n,
+                           double* vorticities, int precision, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  Call c{VPM_OP_VORTICITY_FIELD_AT, targets, m, positions, strengths, radii, nullptr, n,
+         vorticities, nullptr, 0, workspace, workspace_bytes, static_cast<cudaStream_t>(stream)};
+  return dispatch(c, precision);
+}
+
+int vpm_strength_gradients(const double* positions, const double* strengths,
+                           const double* radii, int64_t n, double* dalpha_dt, int precision,
+                           void* workspace, size_t workspace_bytes, void* stream) {
+  Call c{VPM_OP_STRENGTH_GRADIENTS, nullptr, n, positions, strengths, radii, nullptr, n,
+         dalpha_dt, nullptr, 0, workspace, workspace_bytes, static_cast<cudaStream_t>(stream)};
+  return dispatch(c, precision);
+}
+
+int vpm_strength_gradients_pse(const double* positions, const double* strengths,
+                               const double* radii, const double* viscosities, int64_t n,
+                               double* dalpha_dt, int precision, void* workspace,
+                               size_t workspace_bytes, void* stream) {
+  Call c{VPM_OP_STRENGTH_GRADIENTS_PSE, nullptr, n, positions, strengths, radii, viscosities, n,
+         dalpha_dt, nullptr, 0, workspace, workspace_bytes, static_cast<cudaStream_t>(stream)};
+  return dispatch(c, precision);
+}
+
+int vpm_total_kinetic_energy(const double* positions, const double* strengths,
+                             const double* radii, int64_t n, double* energy, int precision,
+                             void* workspace, size_t workspace_bytes, void* stream) {
+  if (!energy) return fail(VPM_ERR_ARG, "null output pointer");
+  Call c{VPM_OP_TOTAL_KINETIC_ENERGY, nullptr, n, positions, strengths, radii, nullptr, n,
+         energy, nullptr, 0, workspace, workspace_bytes, static_cast<cudaStream_t>(stream)};
+  return dispatch(c, precision);
+}
+
+int vpm_total_helicity(const double* positions, const double* strengths, const double* radii,
+                       int64_t n, int ref_extra_4pi, double* helicity, int precision,
+                       void* workspace, size_t workspace_bytes, void* stream) {
+  if (!helicity) return fail(VPM_ERR_ARG, "null output pointer");
+  Call c{VPM_OP_TOTAL_HELICITY, nullptr, n, positions, strengths, radii, nullptr, n,
+         helicity, nullptr, ref_extra_4pi, workspace, workspace_bytes,
+         static_cast<cudaStream_t>(stream)};
+  return dispatch(c, precision);
+}
+
+int vpm_total_enstrophy(const double* positions, const double* strengths, const double* radii,
+                        int64_t n, int ref_extra_4pi, double* enstrophy, int precision,
+                        void* workspace, size_t workspace_bytes, void* stream) {
+  if (!enstrophy) return fail(VPM_ERR_ARG, "null output pointer");
+  Call c{VPM_OP_TOTAL_ENSTROPHY, nullptr, n, positions, strengths, radii, nullptr, n,
+         enstrophy, nullptr, ref_extra_4pi, workspace, workspace_bytes,
+         static_cast<cudaStream_t>(stream)};
+  return dispatch(c, precision);
+}
+
+int vpm_velocity_and_strength_gradients(const double* positions, const double* strengths,
+                                        const double* radii, int64_t n, double* velocities,
+                                        double* dalpha_dt, int precision, void* workspace,
+                                        size_t workspace_bytes, void* stream) {
+  Call c{VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS, nullptr, n, positions, strengths, radii,
+         nullptr, n, velocities, dalpha_dt, 0, workspace, workspace_bytes,
+         static_cast<cudaStream_t>(stream)};
+  return dispatch(c, precision);
+}
+
+size_t vpm_record_bytes(int precision) {
+  switch (precision) {
+    case VPM_FP64:
+      return sizeof(Rec<double>);
+    case VPM_FP32C:
+    case VPM_FP32C_REFINED:
+      return sizeof(Rec<float>);
+    default:
+      fail(VPM_ERR_ARG, "unknown precision");
+      return 0;
+  }
+}
+
+int vpm_pack_records(const double* positions, const double* strengths, const double* radii,
+                     const double* viscosities, int64_t n, int precision, void* records,
+                     void* stream) {
+  if (n < 0) return fail(VPM_ERR_ARG, "negative size");
+  if (n > 0 && (!positions || !strengths || !radii || !records))
+    return fail(VPM_ERR_ARG, "null pointer");
+  if (reinterpret_cast<uintptr_t>(records) % 16 != 0)
+    return fail(VPM_ERR_ALIGN, "records must be 16-byte aligned");
+  int rc = check_arch();
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (precision == VPM_FP64)
+    return pack<double>(positions, strengths, radii, viscosities, n,
+                        static_cast<Rec<double>*>(records), st);
+  if (precision == VPM_FP32C || precision == VPM_FP32C_REFINED)
+    return pack<float>(positions, strengths, radii, viscosities, n,
+                       static_cast<Rec<float>*>(records), st);
+  return fail(VPM_ERR_ARG, "unknown precision");
+}
+
+int vpm_sweep_records(int op, const void* records, int64_t n, int64_t target_begin, int64_t m,
+                      int ref_extra_4pi, double* out, double* out2, int precision,
+                      void* workspace, size_t workspace_bytes, void* stream) {
+  Call c{op, nullptr, m, nullptr, nullptr, nullptr, nullptr, n, out, out2, ref_extra_4pi,
+         workspace, workspace_bytes, static_cast<cudaStream_t>(stream)};
+  c.records = records;
+  c.tgt_begin = target_begin;
+  if (n > 0 && !records) return fail(VPM_ERR_ARG, "null records pointer");
+  return dispatch(c, precision);
+}
+
+int vpm_launch_fma_peak(int fp64, int blocks, int threads, int iters, void* sink, void* stream) {
+  if (blocks <= 0 || threads <= 0 || threads > 1024 || iters <= 0 || !sink)
+    return fail(VPM_ERR_ARG, "bad fma peak launch arguments");
+  int rc = check_arch();
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (fp64)
+    fma_peak_kernel<double><<<blocks, threads, 0, st>>>(iters, static_cast<double*>(sink));
+  else
+    fma_peak_kernel<float><<<blocks, threads, 0, st>>>(iters, static_cast<float*>(sink));
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? VPM_OK : cuda_fail(e, "fma peak launch");
+}
+
+}  // extern "C"

@@ -48,6 +48,10 @@ _SIGS = {
     "oracle_cpu_total_kinetic_energy": ([_D, _D, _D, _I64], ctypes.c_double),
     "oracle_cpu_total_helicity": ([_D, _D, _D, _I64], ctypes.c_double),
     "oracle_cpu_total_enstrophy": ([_D, _D, _D, _I64], ctypes.c_double),
+    "oracle_gpu_selfinduced_velocity_range": ([_D, _D, _D, _I64, _I64, _I64, _D], None),
+    "oracle_gpu_strength_gradients_range": ([_D, _D, _D, _I64, _I64, _I64, _D], None),
+    "oracle_cpu_selfinduced_velocity_range": ([_D, _D, _D, _I64, _I64, _I64, _D], None),
+    "oracle_cpu_strength_gradients_range": ([_D, _D, _D, _I64, _I64, _I64, _D], None),
     "oracle_num_threads": ([], ctypes.c_int),
     "oracle_set_num_threads": ([ctypes.c_int], None),
 }
@@ -115,6 +119,20 @@ class _Module:
         x, a, s = _f64(positions, 3), _f64(strengths, 3), _f64(radii)
         out = np.zeros_like(x)
         self._fn("strength_gradients")(_p(x), _p(a), _p(s), len(x), _p(out))
+        return out
+
+    def selfinduced_velocity_range(self, positions, strengths, radii, t0, t1):
+        """Self-induced velocity of targets [t0, t1) against all particles."""
+        x, a, s = _f64(positions, 3), _f64(strengths, 3), _f64(radii)
+        out = np.zeros((t1 - t0, 3))
+        self._fn("selfinduced_velocity_range")(_p(x), _p(a), _p(s), len(x), t0, t1, _p(out))
+        return out
+
+    def strength_gradients_range(self, positions, strengths, radii, t0, t1):
+        """Stretching of targets [t0, t1) against all particles."""
+        x, a, s = _f64(positions, 3), _f64(strengths, 3), _f64(radii)
+        out = np.zeros((t1 - t0, 3))
+        self._fn("strength_gradients_range")(_p(x), _p(a), _p(s), len(x), t0, t1, _p(out))
         return out
 
     def get_strength_gradients_PSE(self, positions, strengths, radii, viscosities):

@@ -85,10 +85,11 @@ void oracle_gpu_induced_velocity_at(const double* tgt, int64_t m, const double* 
 
 /* get_selfinduced_velocity_kernel, ParticlesPhysicsCuda.py:133-191: j != i, pair core
  * (sigma_i + sigma_j)/2, no r^2 threshold. */
-void oracle_gpu_selfinduced_velocity(const double* pos, const double* str, const double* rad,
-                                     int64_t n, double* out) {
+void oracle_gpu_selfinduced_velocity_range(const double* pos, const double* str,
+                                           const double* rad, int64_t n, int64_t t0, int64_t t1,
+                                           double* out) {
 #pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < n; ++i) {
+  for (int64_t i = t0; i < t1; ++i) {
     double ux = 0.0, uy = 0.0, uz = 0.0;
     const double tx = pos[3 * i], ty = pos[3 * i + 1], tz = pos[3 * i + 2];
     const double ti = rad[i];
@@ -105,10 +106,15 @@ void oracle_gpu_selfinduced_velocity(const double* pos, const double* str, const
       uy -= q * (rz * ax - rx * az);
       uz -= q * (rx * ay - ry * ax);
     }
-    out[3 * i] = ONE_OVER_FOUR_PI * ux;
-    out[3 * i + 1] = ONE_OVER_FOUR_PI * uy;
-    out[3 * i + 2] = ONE_OVER_FOUR_PI * uz;
+    out[3 * (i - t0)] = ONE_OVER_FOUR_PI * ux;
+    out[3 * (i - t0) + 1] = ONE_OVER_FOUR_PI * uy;
+    out[3 * (i - t0) + 2] = ONE_OVER_FOUR_PI * uz;
   }
+}
+
+void oracle_gpu_selfinduced_velocity(const double* pos, const double* str, const double* rad,
+                                     int64_t n, double* out) {
+  oracle_gpu_selfinduced_velocity_range(pos, str, rad, n, 0, n, out);
 }
 
 /* get_vorticity_field_at_kernel_simplified, ParticlesPhysicsCuda.py:291-346 (the kernel
@@ -142,10 +148,11 @@ void oracle_gpu_vorticity_field_at(const double* tgt, int64_t m, const double* p
 
 /* get_strength_gradients_kernel, ParticlesPhysicsCuda.py:375-445: vortex stretching in the
  * transpose scheme, j != i, pair core (sigma_i + sigma_j)/2. */
-void oracle_gpu_strength_gradients(const double* pos, const double* str, const double* rad,
-                                   int64_t n, double* out) {
+void oracle_gpu_strength_gradients_range(const double* pos, const double* str,
+                                         const double* rad, int64_t n, int64_t t0, int64_t t1,
+                                         double* out) {
 #pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < n; ++i) {
+  for (int64_t i = t0; i < t1; ++i) {
     const double ri = rad[i];
     const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
     const double bx = str[3 * i], by = str[3 * i + 1], bz = str[3 * i + 2];
@@ -168,10 +175,15 @@ void oracle_gpu_strength_gradients(const double* pos, const double* str, const d
       gy += (f1 * c1y + f2 * d3 * ry) * ONE_OVER_FOUR_PI;
       gz += (f1 * c1z + f2 * d3 * rz) * ONE_OVER_FOUR_PI;
     }
-    out[3 * i] = gx;
-    out[3 * i + 1] = gy;
-    out[3 * i + 2] = gz;
+    out[3 * (i - t0)] = gx;
+    out[3 * (i - t0) + 1] = gy;
+    out[3 * (i - t0) + 2] = gz;
   }
+}
+
+void oracle_gpu_strength_gradients(const double* pos, const double* str, const double* rad,
+                                   int64_t n, double* out) {
+  oracle_gpu_strength_gradients_range(pos, str, rad, n, 0, n, out);
 }
 
 /* get_strength_gradients_PSE_kernel, ParticlesPhysicsCuda.py:478-530: PSE diffusion with
@@ -316,10 +328,11 @@ void oracle_cpu_induced_velocity_at(const double* tgt, int64_t m, const double* 
 }
 
 /* get_selfinduced_velocity, ParticlesPhysics.py:82-143: core sigma_i of the TARGET. */
-void oracle_cpu_selfinduced_velocity(const double* pos, const double* str, const double* rad,
-                                     int64_t n, double* out) {
+void oracle_cpu_selfinduced_velocity_range(const double* pos, const double* str,
+                                           const double* rad, int64_t n, int64_t t0, int64_t t1,
+                                           double* out) {
 #pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < n; ++i) {
+  for (int64_t i = t0; i < t1; ++i) {
     double ux = 0.0, uy = 0.0, uz = 0.0;
     const double tx = pos[3 * i], ty = pos[3 * i + 1], tz = pos[3 * i + 2];
     const double s = rad[i];
@@ -335,10 +348,15 @@ void oracle_cpu_selfinduced_velocity(const double* pos, const double* str, const
       uy -= q * (rz * ax - rx * az);
       uz -= q * (rx * ay - ry * ax);
     }
-    out[3 * i] = ux * ONE_OVER_FOUR_PI;
-    out[3 * i + 1] = uy * ONE_OVER_FOUR_PI;
-    out[3 * i + 2] = uz * ONE_OVER_FOUR_PI;
+    out[3 * (i - t0)] = ux * ONE_OVER_FOUR_PI;
+    out[3 * (i - t0) + 1] = uy * ONE_OVER_FOUR_PI;
+    out[3 * (i - t0) + 2] = uz * ONE_OVER_FOUR_PI;
   }
+}
+
+void oracle_cpu_selfinduced_velocity(const double* pos, const double* str, const double* rad,
+                                     int64_t n, double* out) {
+  oracle_cpu_selfinduced_velocity_range(pos, str, rad, n, 0, n, out);
 }
 
 /* get_vorticity_field_at, ParticlesPhysics.py:212-262: full zeta/q regularised kernel. */
@@ -376,6 +394,12 @@ void oracle_cpu_vorticity_field_at(const double* tgt, int64_t m, const double* p
 void oracle_cpu_strength_gradients(const double* pos, const double* str, const double* rad,
                                    int64_t n, double* out) {
   oracle_gpu_strength_gradients(pos, str, rad, n, out);
+}
+
+void oracle_cpu_strength_gradients_range(const double* pos, const double* str,
+                                         const double* rad, int64_t n, int64_t t0, int64_t t1,
+                                         double* out) {
+  oracle_gpu_strength_gradients_range(pos, str, rad, n, t0, t1, out);
 }
 
 /* get_strength_gradients_PSE, ParticlesPhysics.py:319-382: viscosity (nu_i + nu_j)/2 and
