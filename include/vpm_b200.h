@@ -131,7 +131,7 @@ int vpm_velocity_and_strength_gradients(const double* positions, const double* s
                                         size_t workspace_bytes, void* stream);
 
 /* ---- pre-packed records (device-resident state, target shards) ----------------------- */
-/* Bytes of one packed particle record: 32 (FP32 forms) or 64 (VPM_FP64). */
+/* Bytes of one packed particle record (64; FP32 records hold every value twice). */
 size_t vpm_record_bytes(int precision);
 /* Pack n particles from the reference layout into records {x,y,z,sigma,ax,ay,az,nu} of the
  * compute precision (viscosities may be NULL: nu = 0).  `records` is 16-byte aligned. */

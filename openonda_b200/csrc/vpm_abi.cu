@@ -37,9 +37,15 @@ size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 // ---- kernel configurations -----------------------------------------------------------
 template <class T>
 struct Cfg;
+#ifndef VPM_FP32_R
+#define VPM_FP32_R 4
+#endif
+#ifndef VPM_FP32_THREADS
+#define VPM_FP32_THREADS 128
+#endif
 template <>
-struct Cfg<float> {
-  static constexpr int R = 4, THREADS = 128, TILE = 256, STAGES = 2;
+struct Cfg<float2> {
+  static constexpr int R = VPM_FP32_R, THREADS = VPM_FP32_THREADS, TILE = 256, STAGES = 2;
 };
 template <>
 struct Cfg<double> {
@@ -101,7 +107,7 @@ template <class Op, class T>
 struct Sweep {
   using C = Cfg<T>;
   static constexpr int NV = Op::NV;
-  static constexpr size_t kSmem = size_t(C::STAGES) * C::TILE * sizeof(Rec<T>);
+  static constexpr size_t kSmem = sweep_smem_bytes<T, Op::NV, C::R, C::THREADS, C::TILE, C::STAGES>();
   static void* kernel() {
     return reinterpret_cast<void*>(&sweep_kernel<Op, T, C::R, C::THREADS, C::TILE, C::STAGES>);
   }
@@ -120,6 +126,11 @@ struct Sweep {
       if (it != g_occ.end()) {
         occ = it->second;
       } else {
+        if (kSmem > 48 * 1024) {
+          cudaError_t e = cudaFuncSetAttribute(kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               int(kSmem));
+          if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(max dynamic smem)");
+        }
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel(),
                                                                       C::THREADS, kSmem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
@@ -173,23 +184,29 @@ struct Sweep {
 };
 
 // ---- pack kernels ----------------------------------------------------------------------
-template <class T>
+__device__ __forceinline__ void set_elem(double& e, double v) { e = v; }
+__device__ __forceinline__ void set_elem(float2& e, double v) {
+  const float f = float(v);
+  e = make_float2(f, f);
+}
+
+template <class E>
 __global__ void pack_particles_kernel(const double* __restrict__ pos,
                                       const double* __restrict__ str,
                                       const double* __restrict__ rad,
                                       const double* __restrict__ nu, int64_t n,
-                                      Rec<T>* __restrict__ out) {
+                                      Rec<E>* __restrict__ out) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  Rec<T> r;
-  r.x = T(pos[3 * i]);
-  r.y = T(pos[3 * i + 1]);
-  r.z = T(pos[3 * i + 2]);
-  r.s = rad ? T(rad[i]) : T(0);
-  r.ax = str ? T(str[3 * i]) : T(0);
-  r.ay = str ? T(str[3 * i + 1]) : T(0);
-  r.az = str ? T(str[3 * i + 2]) : T(0);
-  r.nu = nu ? T(nu[i]) : T(0);
+  Rec<E> r;
+  set_elem(r.x, pos[3 * i]);
+  set_elem(r.y, pos[3 * i + 1]);
+  set_elem(r.z, pos[3 * i + 2]);
+  set_elem(r.s, rad ? rad[i] : 0.0);
+  set_elem(r.ax, str ? str[3 * i] : 0.0);
+  set_elem(r.ay, str ? str[3 * i + 1] : 0.0);
+  set_elem(r.az, str ? str[3 * i + 2] : 0.0);
+  set_elem(r.nu, nu ? nu[i] : 0.0);
   out[i] = r;
 }
 
@@ -238,19 +255,19 @@ __global__ void finalize_vec_kernel(const double* __restrict__ part, int splits,
     out[3 * i + 1] = v[1] * c;
     out[3 * i + 2] = v[2] * c;
   } else if constexpr (KIND == FIN_PSE) {
-    const double c = 105.0 * double(tgt[i].nu) * kOneOver4Pi;
+    const double c = 105.0 * elem(tgt[i].nu) * kOneOver4Pi;
     out[3 * i] = v[0] * c;
     out[3 * i + 1] = v[1] * c;
     out[3 * i + 2] = v[2] * c;
   } else {
     constexpr int o = (KIND == FIN_VELSTRETCH) ? 3 : 0;
     double* so = (KIND == FIN_VELSTRETCH) ? out2 : out;
+    const double bx = elem(tgt[i].ax), by = elem(tgt[i].ay), bz = elem(tgt[i].az);
     if constexpr (KIND == FIN_VELSTRETCH) {
       out[3 * i] = -v[0] * kOneOver4Pi;
       out[3 * i + 1] = -v[1] * kOneOver4Pi;
       out[3 * i + 2] = -v[2] * kOneOver4Pi;
     }
-    const double bx = double(tgt[i].ax), by = double(tgt[i].ay), bz = double(tgt[i].az);
     const double Ax = v[o], Ay = v[o + 1], Az = v[o + 2];
     so[3 * i] = (by * Az - bz * Ay + 3.0 * v[o + 3]) * kOneOver4Pi;
     so[3 * i + 1] = (bz * Ax - bx * Az + 3.0 * v[o + 4]) * kOneOver4Pi;
@@ -270,7 +287,7 @@ finalize_dot_kernel(const double* __restrict__ part, int splits, int64_t m,
   for (int64_t i = threadIdx.x; i < m; i += kReduceThreads) {
     double v[3];
     sum_splits<3>(part, splits, m, i, v);
-    acc += double(tgt[i].ax) * v[0] + double(tgt[i].ay) * v[1] + double(tgt[i].az) * v[2];
+    acc += elem(tgt[i].ax) * v[0] + elem(tgt[i].ay) * v[1] + elem(tgt[i].az) * v[2];
   }
   red[threadIdx.x] = acc;
   __syncthreads();
@@ -462,7 +479,8 @@ int run(const Call& c) {
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
       rc = Sweep<typename O::VelStretch, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
       if (!rc)
-        rc = finalize_vec<T, FIN_VELSTRETCH, 9>(part, p.splits, c.m, tgt, c.out, c.out2, c.st);
+        rc = finalize_vec<T, FIN_VELSTRETCH, O::VelStretch::NV>(part, p.splits, c.m, tgt, c.out,
+                                                               c.out2, c.st);
       return rc;
     case VPM_OP_TOTAL_KINETIC_ENERGY:
     case VPM_OP_TOTAL_HELICITY:
@@ -513,9 +531,9 @@ int dispatch(const Call& c, int precision) {
     case VPM_FP64:
       return run<double, false>(c);
     case VPM_FP32C:
-      return run<float, false>(c);
+      return run<float2, false>(c);
     case VPM_FP32C_REFINED:
-      return run<float, true>(c);
+      return run<float2, true>(c);
     default:
       return fail(VPM_ERR_ARG, "unknown precision " + std::to_string(precision));
   }
@@ -574,10 +592,10 @@ size_t vpm_workspace_bytes(int op, int precision, int64_t m, int64_t n) {
       rc = workspace_for<double, false>(op, m, n, &L, &p);
       break;
     case VPM_FP32C:
-      rc = workspace_for<float, false>(op, m, n, &L, &p);
+      rc = workspace_for<float2, false>(op, m, n, &L, &p);
       break;
     case VPM_FP32C_REFINED:
-      rc = workspace_for<float, true>(op, m, n, &L, &p);
+      rc = workspace_for<float2, true>(op, m, n, &L, &p);
       break;
     default:
       fail(VPM_ERR_ARG, "unknown precision");
@@ -595,10 +613,10 @@ int vpm_plan_info(int op, int precision, int64_t m, int64_t n, int64_t* target_b
       rc = plan_op<double, false>(op, m, n, &p);
       break;
     case VPM_FP32C:
-      rc = plan_op<float, false>(op, m, n, &p);
+      rc = plan_op<float2, false>(op, m, n, &p);
       break;
     case VPM_FP32C_REFINED:
-      rc = plan_op<float, true>(op, m, n, &p);
+      rc = plan_op<float2, true>(op, m, n, &p);
       break;
     default:
       return fail(VPM_ERR_ARG, "unknown precision");
@@ -699,7 +717,7 @@ size_t vpm_record_bytes(int precision) {
       return sizeof(Rec<double>);
     case VPM_FP32C:
     case VPM_FP32C_REFINED:
-      return sizeof(Rec<float>);
+      return sizeof(Rec<float2>);
     default:
       fail(VPM_ERR_ARG, "unknown precision");
       return 0;
@@ -721,8 +739,8 @@ int vpm_pack_records(const double* positions, const double* strengths, const dou
     return pack<double>(positions, strengths, radii, viscosities, n,
                         static_cast<Rec<double>*>(records), st);
   if (precision == VPM_FP32C || precision == VPM_FP32C_REFINED)
-    return pack<float>(positions, strengths, radii, viscosities, n,
-                       static_cast<Rec<float>*>(records), st);
+    return pack<float2>(positions, strengths, radii, viscosities, n,
+                        static_cast<Rec<float2>*>(records), st);
   return fail(VPM_ERR_ARG, "unknown precision");
 }
 

@@ -1,8 +1,8 @@
 // vpm_common.cuh -- shared device helpers for the VPM pair-sum kernels (sm_100a).
 //
 // * Packed particle record: {x, y, z, sigma | ax, ay, az, nu} in the compute precision
-//   (32 B in FP32, 64 B in FP64).  A tile of consecutive records is one contiguous byte
-//   range, so it moves into shared memory with a single bulk-async (TMA) copy.
+//   (64 B).  A tile of consecutive records is one contiguous byte range, so it moves into
+//   shared memory with a single bulk-async (TMA) copy.
 // * Bulk-async copy global -> shared completing on an mbarrier (cp.async.bulk, no
 //   multicast: every load reads this GPU's own memory).
 // * mbarrier waits are bounded by %globaltimer: after VPM_WAIT_LIMIT_NS the wait gives up,
@@ -23,13 +23,16 @@ constexpr int VPM_DEVERR_WAIT_TIMEOUT = 1;
 
 constexpr unsigned long long VPM_WAIT_LIMIT_NS = 1000000000ull;  // 1 s
 
-template <class T>
-struct alignas(sizeof(T) * 4) Rec {
-  T x, y, z, s;
-  T ax, ay, az, nu;
+// Packed particle record.  E = double (FP64 path) or float2 (FP32 path, every value stored
+// twice as {v, v} so a 16-byte shared-memory load yields two broadcast operand pairs for the
+// paired FP32 instructions).  Both forms are 64 bytes.
+template <class E>
+struct alignas(16) Rec {
+  E x, y, z, s;
+  E ax, ay, az, nu;
 };
-static_assert(sizeof(Rec<float>) == 32, "FP32 record is 32 B");
 static_assert(sizeof(Rec<double>) == 64, "FP64 record is 64 B");
+static_assert(sizeof(Rec<float2>) == 64, "FP32 record is 64 B");
 
 // Device error word.  The library is compiled as one translation unit (vpm_abi.cu
 // includes every kernel header), so this is the only instance.
@@ -93,23 +96,6 @@ __device__ __forceinline__ void bulk_load_g2s(void* smem_dst, const void* gmem_s
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
       ::"r"(smem_addr(smem_dst)), "l"(gmem_src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
-}
-
-// Reciprocal square root: hardware approximation in FP32 (optionally refined by one
-// Newton-Raphson step, y <- y + y (1/2 - x y^2 / 2)); CUDA's rsqrt() in FP64.
-template <bool REFINE>
-__device__ __forceinline__ float rsqrt_t(float x) {
-  float y = rsqrtf(x);
-  if constexpr (REFINE) {
-    const float hx = 0.5f * x;
-    const float e = fmaf(-(hx * y), y, 0.5f);
-    y = fmaf(y, e, y);
-  }
-  return y;
-}
-template <bool REFINE>
-__device__ __forceinline__ double rsqrt_t(double x) {
-  return rsqrt(x);
 }
 
 }  // namespace vpm

@@ -1,7 +1,9 @@
 // vpm_pairs.cuh -- per-pair operators of the VPM all-pairs sums.
 //
-// Each operator adds one source particle's contribution to one target's partial sums.
-// All kernels of the reference are written here in the sigma-symmetric rsqrt form
+// Each operator adds one source particle's contribution to the partial sums of one "lane"
+// of targets: one FP64 target (V = double) or two FP32 targets (V = float2, paired FP32
+// instructions).  All kernels of the reference are written in the sigma-symmetric rsqrt
+// form
 //     x = r^2 + s^2,  y = x^(-1/2)
 // where s is the pair core (sigma_i + sigma_j)/2 for self sums and sigma_j for probes:
 //
@@ -17,7 +19,10 @@
 // target in the finalize pass.  The stretching term a_i x a_j is summed as
 //   sum_j g (a_i x a_j) = a_i x sum_j g (a_j - a_i),
 // which is exact in exact arithmetic, vanishes identically for j == i and keeps the
-// partial sum small when neighbouring strengths are nearly parallel.
+// partial sum small when neighbouring strengths are nearly parallel.  In the stretching-only
+// operator the triple product a_i . (r x a_j) is evaluated as r . (d x a_i) with
+// d = a_j - a_i (equal since a_i . (r x a_i) = 0; same cost there); the fused operator
+// reuses the velocity's r x a_j instead, which measured equally accurate and is cheaper.
 //
 // References (OpenONDA/solvers/VPM/ParticlesPhysicsCuda.py):
 //   OpVel      get_selfinduced_velocity_kernel      :133-191
@@ -30,23 +35,25 @@
 //   (helicity, :673-750, is  -a_i . sum_j g (r x a_j), i.e. a by-product of OpVel)
 #pragma once
 
-#include "vpm_common.cuh"
+#include "vpm_lanes.cuh"
 
 namespace vpm {
 
-template <class T>
+template <class V>
 struct Src {
-  T x, y, z, s, ax, ay, az, nu;
+  V x, y, z, s, ax, ay, az, nu;
 };
 
-template <class T>
-__device__ __forceinline__ Src<T> load_src(const Rec<T>& r);
+template <class V>
+__device__ __forceinline__ Src<V> load_src(const Rec<V>& r);
 
 template <>
-__device__ __forceinline__ Src<float> load_src<float>(const Rec<float>& r) {
+__device__ __forceinline__ Src<float2> load_src<float2>(const Rec<float2>& r) {
   const float4* p = reinterpret_cast<const float4*>(&r);
-  const float4 a = p[0], b = p[1];
-  return Src<float>{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  const float4 a = p[0], b = p[1], c = p[2], d = p[3];
+  return Src<float2>{make_float2(a.x, a.y), make_float2(a.z, a.w), make_float2(b.x, b.y),
+                     make_float2(b.z, b.w), make_float2(c.x, c.y), make_float2(c.z, c.w),
+                     make_float2(d.x, d.y), make_float2(d.z, d.w)};
 }
 
 template <>
@@ -56,36 +63,44 @@ __device__ __forceinline__ Src<double> load_src<double>(const Rec<double>& r) {
   return Src<double>{a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y};
 }
 
-// Per-target registers shared by all operators.
-template <class T>
+// Per-lane target registers shared by all operators.
+template <class V>
 struct Tgt {
-  T x, y, z, hs;   // position, half core
-  T ax, ay, az;    // strength
+  V x, y, z, hs;  // position, half core
+  V ax, ay, az;   // strength
 };
 
-template <class T>
-__device__ __forceinline__ Tgt<T> make_tgt(const Rec<T>& r) {
-  return Tgt<T>{r.x, r.y, r.z, T(0.5) * r.s, r.ax, r.ay, r.az};
+// `r` points at the lane's records: one for FP64, two (lane 0, lane 1) for FP32.
+__device__ __forceinline__ Tgt<double> make_tgt(const Rec<double>* const* r) {
+  const Rec<double>& a = *r[0];
+  return Tgt<double>{a.x, a.y, a.z, 0.5 * a.s, a.ax, a.ay, a.az};
+}
+__device__ __forceinline__ Tgt<float2> make_tgt(const Rec<float2>* const* r) {
+  const Rec<float2>& a = *r[0];
+  const Rec<float2>& b = *r[1];
+  return Tgt<float2>{make_float2(a.x.x, b.x.x),   make_float2(a.y.x, b.y.x),
+                     make_float2(a.z.x, b.z.x),   make_float2(0.5f * a.s.x, 0.5f * b.s.x),
+                     make_float2(a.ax.x, b.ax.x), make_float2(a.ay.x, b.ay.x),
+                     make_float2(a.az.x, b.az.x)};
 }
 
 // ---- self-induced velocity: U += g (r x a_j) ------------------------------------------
-template <class T, bool REFINE>
+template <class V, bool REFINE>
 struct OpVel {
   static constexpr int NV = 3;
-  static constexpr bool EXCLUDE_SELF = false;
-  __device__ __forceinline__ static void pair(const Tgt<T>& t, T* acc, const Src<T>& s,
-                                              int64_t, int64_t) {
-    const T rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const T sg = fma(s.s, T(0.5), t.hs);
-    const T s2 = sg * sg;
-    const T x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
-    const T y = rsqrt_t<REFINE>(x);
-    const T y2 = y * y;
-    const T y5 = (y2 * y2) * y;
-    const T g = fma(T(1.5), s2, x) * y5;
-    const T cx = fma(ry, s.az, -(rz * s.ay));
-    const T cy = fma(rz, s.ax, -(rx * s.az));
-    const T cz = fma(rx, s.ay, -(ry * s.ax));
+  __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
+                                              const int64_t*, int64_t) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    const V sg = fma(s.s, splat<V>(0.5), t.hs);
+    const V s2 = sg * sg;
+    const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
+    const V y = rsqrt_lane<REFINE>(x);
+    const V y2 = y * y;
+    const V y5 = (y2 * y2) * y;
+    const V g = fma(splat<V>(1.5), s2, x) * y5;
+    const V cx = fma(ry, s.az, -(rz * s.ay));
+    const V cy = fma(rz, s.ax, -(rx * s.az));
+    const V cz = fma(rx, s.ay, -(ry * s.ax));
     acc[0] = fma(g, cx, acc[0]);
     acc[1] = fma(g, cy, acc[1]);
     acc[2] = fma(g, cz, acc[2]);
@@ -93,23 +108,21 @@ struct OpVel {
 };
 
 // ---- probe velocity: source core sigma_j, pairs with r^2 <= 1e-8 skipped ----------------
-template <class T, bool REFINE>
+template <class V, bool REFINE>
 struct OpVelAt {
   static constexpr int NV = 3;
-  static constexpr bool EXCLUDE_SELF = false;
-  __device__ __forceinline__ static void pair(const Tgt<T>& t, T* acc, const Src<T>& s,
-                                              int64_t, int64_t) {
-    const T rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const T r2 = fma(rx, rx, fma(ry, ry, rz * rz));
-    const T s2 = s.s * s.s;
-    const T y = rsqrt_t<REFINE>(r2 + s2);
-    const T y2 = y * y;
-    const T y5 = (y2 * y2) * y;
-    T g = fma(T(2.5), s2, r2) * y5;
-    g = (r2 > T(kRefEps)) ? g : T(0);
-    const T cx = fma(ry, s.az, -(rz * s.ay));
-    const T cy = fma(rz, s.ax, -(rx * s.az));
-    const T cz = fma(rx, s.ay, -(ry * s.ax));
+  __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
+                                              const int64_t*, int64_t) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    const V r2 = fma(rx, rx, fma(ry, ry, rz * rz));
+    const V s2 = s.s * s.s;
+    const V y = rsqrt_lane<REFINE>(r2 + s2);
+    const V y2 = y * y;
+    const V y5 = (y2 * y2) * y;
+    const V g = keep_if_gt(r2, kRefEps, fma(splat<V>(2.5), s2, r2) * y5);
+    const V cx = fma(ry, s.az, -(rz * s.ay));
+    const V cy = fma(rz, s.ax, -(rx * s.az));
+    const V cz = fma(rx, s.ay, -(ry * s.ax));
     acc[0] = fma(g, cx, acc[0]);
     acc[1] = fma(g, cy, acc[1]);
     acc[2] = fma(g, cz, acc[2]);
@@ -117,51 +130,49 @@ struct OpVelAt {
 };
 
 // ---- probe vorticity (zeta kernel only): W += s^4 y^7 a_j, r^2 <= 1e-8 skipped ----------
-template <class T, bool REFINE>
+template <class V, bool REFINE>
 struct OpVortAt {
   static constexpr int NV = 3;
-  static constexpr bool EXCLUDE_SELF = false;
-  __device__ __forceinline__ static void pair(const Tgt<T>& t, T* acc, const Src<T>& s,
-                                              int64_t, int64_t) {
-    const T rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const T r2 = fma(rx, rx, fma(ry, ry, rz * rz));
-    const T s2 = s.s * s.s;
-    const T y = rsqrt_t<REFINE>(r2 + s2);
-    const T y2 = y * y;
-    const T y3 = y2 * y;
-    const T y7 = (y3 * y3) * y;
-    T k = (s2 * s2) * y7;
-    k = (r2 > T(kRefEps)) ? k : T(0);
+  __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
+                                              const int64_t*, int64_t) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    const V r2 = fma(rx, rx, fma(ry, ry, rz * rz));
+    const V s2 = s.s * s.s;
+    const V y = rsqrt_lane<REFINE>(r2 + s2);
+    const V y2 = y * y;
+    const V y3 = y2 * y;
+    const V y7 = (y3 * y3) * y;
+    const V k = keep_if_gt(r2, kRefEps, (s2 * s2) * y7);
     acc[0] = fma(k, s.ax, acc[0]);
     acc[1] = fma(k, s.ay, acc[1]);
     acc[2] = fma(k, s.az, acc[2]);
   }
 };
 
-// ---- stretching (transpose scheme): A += g (a_j - a_i),  B += f (a_i . (r x a_j)) r -----
-template <class T, bool REFINE>
+// ---- stretching (transpose scheme): A += g (a_j - a_i),  B += f (r . (d x a_i)) r -------
+template <class V, bool REFINE>
 struct OpStretch {
   static constexpr int NV = 6;
-  static constexpr bool EXCLUDE_SELF = false;
-  __device__ __forceinline__ static void pair(const Tgt<T>& t, T* acc, const Src<T>& s,
-                                              int64_t, int64_t) {
-    const T rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const T sg = fma(s.s, T(0.5), t.hs);
-    const T s2 = sg * sg;
-    const T x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
-    const T y = rsqrt_t<REFINE>(x);
-    const T y2 = y * y;
-    const T y5 = (y2 * y2) * y;
-    const T t1 = fma(T(1.5), s2, x);
-    const T g = t1 * y5;
-    const T f = (t1 + s2) * (y5 * y2);
-    const T cx = fma(ry, s.az, -(rz * s.ay));
-    const T cy = fma(rz, s.ax, -(rx * s.az));
-    const T cz = fma(rx, s.ay, -(ry * s.ax));
-    acc[0] = fma(g, s.ax - t.ax, acc[0]);
-    acc[1] = fma(g, s.ay - t.ay, acc[1]);
-    acc[2] = fma(g, s.az - t.az, acc[2]);
-    const T h = f * fma(t.ax, cx, fma(t.ay, cy, t.az * cz));
+  __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
+                                              const int64_t*, int64_t) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    const V sg = fma(s.s, splat<V>(0.5), t.hs);
+    const V s2 = sg * sg;
+    const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
+    const V y = rsqrt_lane<REFINE>(x);
+    const V y2 = y * y;
+    const V y5 = (y2 * y2) * y;
+    const V t1 = fma(splat<V>(1.5), s2, x);
+    const V g = t1 * y5;
+    const V f = (t1 + s2) * (y5 * y2);
+    const V dx = s.ax - t.ax, dy = s.ay - t.ay, dz = s.az - t.az;
+    acc[0] = fma(g, dx, acc[0]);
+    acc[1] = fma(g, dy, acc[1]);
+    acc[2] = fma(g, dz, acc[2]);
+    const V wx = fma(dy, t.az, -(dz * t.ay));
+    const V wy = fma(dz, t.ax, -(dx * t.az));
+    const V wz = fma(dx, t.ay, -(dy * t.ax));
+    const V h = f * fma(rx, wx, fma(ry, wy, rz * wz));
     acc[3] = fma(h, rx, acc[3]);
     acc[4] = fma(h, ry, acc[4]);
     acc[5] = fma(h, rz, acc[5]);
@@ -169,32 +180,38 @@ struct OpStretch {
 };
 
 // ---- fused velocity + stretching: U (3), A (3), B (3) ----------------------------------
-template <class T, bool REFINE>
+#ifndef VPM_Y2_RCP
+#define VPM_Y2_RCP 0
+#endif
+template <class V, bool REFINE>
 struct OpVelStretch {
   static constexpr int NV = 9;
-  static constexpr bool EXCLUDE_SELF = false;
-  __device__ __forceinline__ static void pair(const Tgt<T>& t, T* acc, const Src<T>& s,
-                                              int64_t, int64_t) {
-    const T rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const T sg = fma(s.s, T(0.5), t.hs);
-    const T s2 = sg * sg;
-    const T x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
-    const T y = rsqrt_t<REFINE>(x);
-    const T y2 = y * y;
-    const T y5 = (y2 * y2) * y;
-    const T t1 = fma(T(1.5), s2, x);
-    const T g = t1 * y5;
-    const T f = (t1 + s2) * (y5 * y2);
-    const T cx = fma(ry, s.az, -(rz * s.ay));
-    const T cy = fma(rz, s.ax, -(rx * s.az));
-    const T cz = fma(rx, s.ay, -(ry * s.ax));
+  __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
+                                              const int64_t*, int64_t) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    const V sg = fma(s.s, splat<V>(0.5), t.hs);
+    const V s2 = sg * sg;
+    const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
+    const V y = rsqrt_lane<REFINE>(x);
+#if VPM_Y2_RCP
+    const V y2 = (LaneTraits<V>::kLanes == 2) ? rcp_lane(x) : y * y;
+#else
+    const V y2 = y * y;
+#endif
+    const V y5 = (y2 * y2) * y;
+    const V t1 = fma(splat<V>(1.5), s2, x);
+    const V g = t1 * y5;
+    const V f = (t1 + s2) * (y5 * y2);
+    const V cx = fma(ry, s.az, -(rz * s.ay));
+    const V cy = fma(rz, s.ax, -(rx * s.az));
+    const V cz = fma(rx, s.ay, -(ry * s.ax));
     acc[0] = fma(g, cx, acc[0]);
     acc[1] = fma(g, cy, acc[1]);
     acc[2] = fma(g, cz, acc[2]);
     acc[3] = fma(g, s.ax - t.ax, acc[3]);
     acc[4] = fma(g, s.ay - t.ay, acc[4]);
     acc[5] = fma(g, s.az - t.az, acc[5]);
-    const T h = f * fma(t.ax, cx, fma(t.ay, cy, t.az * cz));
+    const V h = f * fma(t.ax, cx, fma(t.ay, cy, t.az * cz));
     acc[6] = fma(h, rx, acc[6]);
     acc[7] = fma(h, ry, acc[7]);
     acc[8] = fma(h, rz, acc[8]);
@@ -202,22 +219,21 @@ struct OpVelStretch {
 };
 
 // ---- PSE diffusion: P += s^7 y^9 (a_j - a_i)  (nu_i applied in finalize) -----------------
-template <class T, bool REFINE>
+template <class V, bool REFINE>
 struct OpPse {
   static constexpr int NV = 3;
-  static constexpr bool EXCLUDE_SELF = false;
-  __device__ __forceinline__ static void pair(const Tgt<T>& t, T* acc, const Src<T>& s,
-                                              int64_t, int64_t) {
-    const T rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const T sg = fma(s.s, T(0.5), t.hs);
-    const T s2 = sg * sg;
-    const T x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
-    const T y = rsqrt_t<REFINE>(x);
-    const T z = sg * y;  // <= 1
-    const T z2 = z * z;
-    const T z4 = z2 * z2;
-    const T z7 = (z4 * z2) * z;
-    const T k = z7 * (y * y);
+  __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
+                                              const int64_t*, int64_t) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    const V sg = fma(s.s, splat<V>(0.5), t.hs);
+    const V s2 = sg * sg;
+    const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
+    const V y = rsqrt_lane<REFINE>(x);
+    const V z = sg * y;  // <= 1
+    const V z2 = z * z;
+    const V z4 = z2 * z2;
+    const V z7 = (z4 * z2) * z;
+    const V k = z7 * (y * y);
     acc[0] = fma(k, s.ax - t.ax, acc[0]);
     acc[1] = fma(k, s.ay - t.ay, acc[1]);
     acc[2] = fma(k, s.az - t.az, acc[2]);
@@ -225,19 +241,18 @@ struct OpPse {
 };
 
 // ---- enstrophy filter sum (all pairs incl. i == j): V += (x + 2.2 s^2) y^3 a_j ---------
-template <class T, bool REFINE>
+template <class V, bool REFINE>
 struct OpEns {
   static constexpr int NV = 3;
-  static constexpr bool EXCLUDE_SELF = false;
-  __device__ __forceinline__ static void pair(const Tgt<T>& t, T* acc, const Src<T>& s,
-                                              int64_t, int64_t) {
-    const T rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const T sg = fma(s.s, T(0.5), t.hs);
-    const T s2 = sg * sg;
-    const T x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
-    const T y = rsqrt_t<REFINE>(x);
-    const T y3 = (y * y) * y;
-    const T k = fma(T(2.2), s2, x) * y3;
+  __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
+                                              const int64_t*, int64_t) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    const V sg = fma(s.s, splat<V>(0.5), t.hs);
+    const V s2 = sg * sg;
+    const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
+    const V y = rsqrt_lane<REFINE>(x);
+    const V y3 = (y * y) * y;
+    const V k = fma(splat<V>(2.2), s2, x) * y3;
     acc[0] = fma(k, s.ax, acc[0]);
     acc[1] = fma(k, s.ay, acc[1]);
     acc[2] = fma(k, s.az, acc[2]);
@@ -245,21 +260,19 @@ struct OpEns {
 };
 
 // ---- kinetic energy (j != i): K += (y + s^2 y^3) a_j + y^3 (r . a_j) r ------------------
-template <class T, bool REFINE>
+template <class V, bool REFINE>
 struct OpKe {
   static constexpr int NV = 3;
-  static constexpr bool EXCLUDE_SELF = true;
-  __device__ __forceinline__ static void pair(const Tgt<T>& t, T* acc, const Src<T>& s,
-                                              int64_t i, int64_t j) {
-    const T rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const T sg = fma(s.s, T(0.5), t.hs);
-    const T s2 = sg * sg;
-    const T x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
-    const T y = rsqrt_t<REFINE>(x);
-    const T y3 = (y * y) * y;
-    T w = fma(s2, y3, y);
-    w = (i == j) ? T(0) : w;
-    const T q = y3 * fma(rx, s.ax, fma(ry, s.ay, rz * s.az));
+  __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
+                                              const int64_t* i, int64_t j) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    const V sg = fma(s.s, splat<V>(0.5), t.hs);
+    const V s2 = sg * sg;
+    const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
+    const V y = rsqrt_lane<REFINE>(x);
+    const V y3 = (y * y) * y;
+    const V w = zero_if_self(fma(s2, y3, y), i, j);
+    const V q = y3 * fma(rx, s.ax, fma(ry, s.ay, rz * s.az));
     acc[0] = fma(q, rx, fma(w, s.ax, acc[0]));
     acc[1] = fma(q, ry, fma(w, s.ay, acc[1]));
     acc[2] = fma(q, rz, fma(w, s.az, acc[2]));

@@ -9,7 +9,8 @@
 // Accumulation: in FP64 the partial sums accumulate directly in double.  In FP32 each
 // target keeps an FP32 accumulator for a window of CW=32 consecutive sources and folds
 // it into an FP64 carry at the end of every window (one DADD per value per 32 pairs), so
-// rounding grows only over 32 terms and the long sum over N sources runs in FP64.
+// rounding grows only over 32 terms and the long sum over N sources runs in FP64.  FP32
+// targets are processed two at a time with the paired FP32 instructions of sm_100.
 //
 // Each (split, value, target) partial is written as FP64 to
 // partial[(split * NV + v) * m + i]; a finalize pass sums the splits in split order, so
@@ -20,28 +21,53 @@
 
 namespace vpm {
 
-constexpr int kCarryWindow = 32;
+#ifndef VPM_CARRY_WINDOW
+#define VPM_CARRY_WINDOW 32
+#endif
+constexpr int kCarryWindow = VPM_CARRY_WINDOW;
 
-template <class T>
+template <class V>
 struct SweepArgs {
-  const Rec<T>* tgt;
+  const Rec<V>* tgt;
   int64_t m;
   int64_t tgt_offset;  // global index of tgt[0] among the sources (self-pair exclusion)
-  const Rec<T>* src;
+  const Rec<V>* src;
   int64_t n;
   int64_t chunk;  // sources per split (multiple of kCarryWindow unless it is the last)
   double* partial;
 };
 
-template <class Op, class T, int R, int THREADS, int TILE, int STAGES>
+// V = double: R FP64 targets per thread.  V = float2: R FP32 targets per thread as R/2
+// packed lanes; FP32 partials are folded into per-target FP64 carries every window.
+#ifndef VPM_SMEM_CARRY
+#define VPM_SMEM_CARRY 0
+#endif
+#ifndef VPM_SRC_UNROLL
+#define VPM_SRC_UNROLL 2
+#endif
+constexpr int kSrcUnroll = VPM_SRC_UNROLL;
+
+// Dynamic shared memory of one block: the source-tile ring, then (FP32 with shared-memory
+// carries) the FP64 carries laid out [value][target][thread] for conflict-free access.
+template <class V, int NV, int R, int THREADS, int TILE, int STAGES>
+constexpr size_t sweep_smem_bytes() {
+  return size_t(STAGES) * TILE * sizeof(Rec<V>) +
+         ((LaneTraits<V>::kLanes == 2 && VPM_SMEM_CARRY) ? size_t(NV) * R * THREADS * 8 : 0);
+}
+
+template <class Op, class V, int R, int THREADS, int TILE, int STAGES>
 __global__ void __launch_bounds__(THREADS)
-sweep_kernel(const SweepArgs<T> a) {
+sweep_kernel(const SweepArgs<V> a) {
   constexpr int NV = Op::NV;
-  constexpr bool kFp32 = sizeof(T) == 4;
-  constexpr uint32_t kRecBytes = sizeof(Rec<T>);
+  constexpr int L = LaneTraits<V>::kLanes;
+  constexpr int P = R / L;
+  constexpr bool kCarry = (L == 2);
+  constexpr bool kSmemCarry = kCarry && VPM_SMEM_CARRY;
+  constexpr uint32_t kRecBytes = sizeof(Rec<V>);
+  static_assert(R % L == 0, "targets per thread must fill whole lanes");
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  Rec<T>* tiles = reinterpret_cast<Rec<T>*>(smem_raw);
+  Rec<V>* tiles = reinterpret_cast<Rec<V>*>(smem_raw);
   __shared__ __align__(8) uint64_t full_bar[STAGES];
 
   const int tid = threadIdx.x;
@@ -51,21 +77,36 @@ sweep_kernel(const SweepArgs<T> a) {
   const int64_t count = (j1 > j0) ? (j1 - j0) : 0;
   const int ntiles = static_cast<int>((count + TILE - 1) / TILE);
 
-  Tgt<T> tg[R];
-  int64_t ti[R];
-  T acc[R][NV];
-  double car[R][NV];
+  Tgt<V> tg[P];
+  int64_t ti[R];  // local target index
+  int64_t gi[R];  // global index among the sources
+  V acc[P][NV];
+  double car[(kCarry && !kSmemCarry) ? R : 1][NV];
+  double* scar = reinterpret_cast<double*>(smem_raw + size_t(STAGES) * TILE * sizeof(Rec<V>));
+  if constexpr (kSmemCarry) {
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    ti[r] = base + r * THREADS + tid;
-    const int64_t il = ti[r] < a.m ? ti[r] : a.m - 1;
-    tg[r] = make_tgt<T>(a.tgt[il]);
+    for (int v = 0; v < NV; ++v)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      acc[r][v] = T(0);
-      car[r][v] = 0.0;
-    }
+      for (int r = 0; r < R; ++r) scar[(v * R + r) * THREADS + tid] = 0.0;
   }
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    const Rec<V>* recs[L];
+#pragma unroll
+    for (int k = 0; k < L; ++k) {
+      const int r = p * L + k;
+      ti[r] = base + r * THREADS + tid;
+      gi[r] = ti[r] + a.tgt_offset;
+      recs[k] = a.tgt + (ti[r] < a.m ? ti[r] : a.m - 1);
+    }
+    tg[p] = make_tgt(recs);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) lane_zero(acc[p][v]);
+  }
+#pragma unroll
+  for (int r = 0; r < ((kCarry && !kSmemCarry) ? R : 1); ++r)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) car[r][v] = 0.0;
 
   if (tid == 0) {
 #pragma unroll
@@ -91,27 +132,38 @@ sweep_kernel(const SweepArgs<T> a) {
   for (int t = 0; t < ntiles; ++t) {
     const int s = t % STAGES;
     const bool ok = mbar_wait_bounded(&full_bar[s], static_cast<uint32_t>((t / STAGES) & 1));
-    const Rec<T>* tile = tiles + s * TILE;
+    const Rec<V>* tile = tiles + s * TILE;
     const int64_t jt = j0 + static_cast<int64_t>(t) * TILE;
-    const int cnt = static_cast<int>((count - static_cast<int64_t>(t) * TILE) < TILE
-                                         ? (count - static_cast<int64_t>(t) * TILE)
-                                         : TILE);
+    const int64_t left = count - static_cast<int64_t>(t) * TILE;
+    const int cnt = static_cast<int>(left < TILE ? left : TILE);
     if (ok) {
       for (int w = 0; w < cnt; w += kCarryWindow) {
         const int e = (w + kCarryWindow < cnt) ? w + kCarryWindow : cnt;
-#pragma unroll 2
+#pragma unroll kSrcUnroll
         for (int j = w; j < e; ++j) {
-          const Src<T> src = load_src<T>(tile[j]);
+          const Src<V> src = load_src<V>(tile[j]);
 #pragma unroll
-          for (int r = 0; r < R; ++r) Op::pair(tg[r], acc[r], src, ti[r] + a.tgt_offset, jt + j);
+          for (int p = 0; p < P; ++p) Op::pair(tg[p], acc[p], src, &gi[p * L], jt + j);
         }
-        if constexpr (kFp32) {
+        if constexpr (kSmemCarry) {
 #pragma unroll
-          for (int r = 0; r < R; ++r) {
+          for (int p = 0; p < P; ++p) {
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-              car[r][v] += static_cast<double>(acc[r][v]);
-              acc[r][v] = T(0);
+#pragma unroll
+              for (int k = 0; k < L; ++k)
+                scar[(v * R + p * L + k) * THREADS + tid] += lane_get(acc[p][v], k);
+              lane_zero(acc[p][v]);
+            }
+          }
+        } else if constexpr (kCarry) {
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+#pragma unroll
+              for (int k = 0; k < L; ++k) car[p * L + k][v] += lane_get(acc[p][v], k);
+              lane_zero(acc[p][v]);
             }
           }
         }
@@ -141,7 +193,13 @@ sweep_kernel(const SweepArgs<T> a) {
     if (ti[r] < a.m) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        const double val = kFp32 ? car[r][v] : static_cast<double>(acc[r][v]);
+        double val;
+        if constexpr (kSmemCarry)
+          val = scar[(v * R + r) * THREADS + tid];
+        else if constexpr (kCarry)
+          val = car[r][v];
+        else
+          val = lane_get(acc[r / L][v], r % L);
         out[static_cast<int64_t>(v) * a.m + ti[r]] = val;
       }
     }
