@@ -32,8 +32,8 @@ sys.path.insert(0, HERE)
 METRIC = "Biot-Savart Gpairs/s at N=1M: FP32-compensated vs FP64 at <=1e-6 rel err"
 UNIT = "Gpairs/s"
 # FP32-pipe work per pair of the fused velocity + stretching sweep:
-# 38 FP32 instructions = 20 FFMA + 12 FMUL + 6 FADD -> 58 flops (FMA = 2), 1 MUFU.RSQ.
-FLOPS_PER_PAIR_FUSED = 58
+# 38 FP32 lane-ops = 19 FFMA + 12 FMUL + 7 FADD -> 57 flops (FMA = 2), 1 MUFU.RSQ.
+FLOPS_PER_PAIR_FUSED = 57
 FP32_OPS_PER_PAIR_FUSED = 38
 L2_FLUSH_BYTES = 512 << 20
 
