@@ -147,6 +147,20 @@ int vpm_sweep_records(int op, const void* records, int64_t n, int64_t target_beg
                       int ref_extra_4pi, double* out, double* out2, int precision,
                       void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- no-allocation variant ------------------------------------------------------------ */
+#define VPM_NOALLOC_MAX_N 32768
+#define VPM_NOALLOC_SCRATCH_BYTES (8u << 20)
+/* Self-induced velocity (same inputs, output and precisions as vpm_selfinduced_velocity) for
+ * callers that may not allocate device memory, e.g. a plugin inside a host application that
+ * owns the GPU's memory through its own pool.  No counterpart in the reference.  It takes no
+ * workspace and calls no allocator: its scratch is a static 8 MiB device array inside the
+ * library (reserved on every GPU that loads it), so n <= VPM_NOALLOC_MAX_N (larger n returns
+ * VPM_ERR_ARG).  All calls share that array: calls that overlap on the GPU race.  The first
+ * call on a device looks up the array's address; make it before any stream capture. */
+int vpm_selfinduced_velocity_noalloc(const double* positions, const double* strengths,
+                                     const double* radii, int64_t n, double* velocities,
+                                     int precision, void* stream);
+
 /* ---- measurement helpers -------------------------------------------------------------- */
 /* FP32 FMA (fp64 != 0: FP64 FMA) throughput kernel: blocks x threads threads each run
  * `iters` iterations of 16 independent FMA chains; one value per thread lands in `sink`

@@ -59,6 +59,7 @@ SIGNATURES = {
     "vpm_record_bytes": ([_I], _SZ),
     "vpm_pack_records": ([_P, _P, _P, _P, _I64, _I, _P, _P], _I),
     "vpm_sweep_records": ([_I, _P, _I64, _I64, _I64, _I, _P, _P, _I, _P, _SZ, _P], _I),
+    "vpm_selfinduced_velocity_noalloc": ([_P, _P, _P, _I64, _P, _I, _P], _I),
     "vpm_launch_fma_peak": ([_I, _I, _I, _I, _P, _P], _I),
 }
 

@@ -112,7 +112,7 @@ struct Sweep {
     return reinterpret_cast<void*>(&sweep_kernel<Op, T, C::R, C::THREADS, C::TILE, C::STAGES>);
   }
 
-  static int plan(int64_t m, int64_t n, Plan* p) {
+  static int plan(int64_t m, int64_t n, Plan* p, size_t max_partial_bytes = kMaxPartialBytes) {
     DevInfo d;
     int rc = device_info(&d);
     if (rc) return rc;
@@ -155,7 +155,7 @@ struct Sweep {
       if (s > 1 && chunk < kMinChunk) break;
       const int64_t se = (n + chunk - 1) / chunk;
       if (se != s) continue;
-      if (size_t(se) * NV * size_t(m) * sizeof(double) > kMaxPartialBytes) break;
+      if (size_t(se) * NV * size_t(m) * sizeof(double) > max_partial_bytes) break;
       const double waves = double(p->tblocks) * se / slots;
       const double eff = waves / std::ceil(waves);
       const double score = eff * (1.0 - 0.003 * (se - 1));
@@ -341,26 +341,26 @@ struct Ops {
 bool is_probe(int op) { return op == VPM_OP_INDUCED_VELOCITY_AT || op == VPM_OP_VORTICITY_FIELD_AT; }
 
 template <class T, bool REFINE>
-int plan_op(int op, int64_t m, int64_t n, Plan* p) {
+int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes) {
   using O = Ops<T, REFINE>;
   switch (op) {
     case VPM_OP_SELFINDUCED_VELOCITY:
     case VPM_OP_TOTAL_HELICITY:
-      return Sweep<typename O::Vel, T>::plan(m, n, p);
+      return Sweep<typename O::Vel, T>::plan(m, n, p, mpb);
     case VPM_OP_INDUCED_VELOCITY_AT:
-      return Sweep<typename O::VelAt, T>::plan(m, n, p);
+      return Sweep<typename O::VelAt, T>::plan(m, n, p, mpb);
     case VPM_OP_VORTICITY_FIELD_AT:
-      return Sweep<typename O::VortAt, T>::plan(m, n, p);
+      return Sweep<typename O::VortAt, T>::plan(m, n, p, mpb);
     case VPM_OP_STRENGTH_GRADIENTS:
-      return Sweep<typename O::Stretch, T>::plan(m, n, p);
+      return Sweep<typename O::Stretch, T>::plan(m, n, p, mpb);
     case VPM_OP_STRENGTH_GRADIENTS_PSE:
-      return Sweep<typename O::Pse, T>::plan(m, n, p);
+      return Sweep<typename O::Pse, T>::plan(m, n, p, mpb);
     case VPM_OP_TOTAL_KINETIC_ENERGY:
-      return Sweep<typename O::Ke, T>::plan(m, n, p);
+      return Sweep<typename O::Ke, T>::plan(m, n, p, mpb);
     case VPM_OP_TOTAL_ENSTROPHY:
-      return Sweep<typename O::Ens, T>::plan(m, n, p);
+      return Sweep<typename O::Ens, T>::plan(m, n, p, mpb);
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
-      return Sweep<typename O::VelStretch, T>::plan(m, n, p);
+      return Sweep<typename O::VelStretch, T>::plan(m, n, p, mpb);
     default:
       return fail(VPM_ERR_ARG, "unknown op " + std::to_string(op));
   }
@@ -384,8 +384,9 @@ Layout layout_for(int op, const Plan& p, int64_t m, int64_t n) {
 }
 
 template <class T, bool REFINE>
-int workspace_for(int op, int64_t m, int64_t n, Layout* L, Plan* p) {
-  int rc = plan_op<T, REFINE>(op, m, n, p);
+int workspace_for(int op, int64_t m, int64_t n, Layout* L, Plan* p,
+                  size_t max_partial_bytes = kMaxPartialBytes) {
+  int rc = plan_op<T, REFINE>(op, m, n, p, max_partial_bytes);
   if (rc) return rc;
   *L = layout_for<T>(op, *p, m, n);
   return VPM_OK;
@@ -408,6 +409,7 @@ struct Call {
   cudaStream_t st;
   const void* records = nullptr;  // pre-packed sources (self sums); null = pack from AoS
   int64_t tgt_begin = 0;          // self sums: targets are records[tgt_begin, tgt_begin + m)
+  size_t max_partial_bytes = kMaxPartialBytes;  // caps the source splits of the plan
 };
 
 template <class T, bool REFINE>
@@ -431,7 +433,7 @@ int run(const Call& c) {
 
   Plan p;
   Layout L;
-  rc = workspace_for<T, REFINE>(c.op, c.m, c.n, &L, &p);
+  rc = workspace_for<T, REFINE>(c.op, c.m, c.n, &L, &p, c.max_partial_bytes);
   if (rc) return rc;
   if (c.ws == nullptr) return fail(VPM_ERR_WORKSPACE, "workspace is null");
   if (reinterpret_cast<uintptr_t>(c.ws) % kAlign != 0)
@@ -539,6 +541,24 @@ int dispatch(const Call& c, int precision) {
   }
 }
 
+// ---- scratch for the no-allocation entry point --------------------------------------------
+// Some callers may not allocate device memory at all: a solver plugin that runs inside a
+// host application which owns the whole GPU memory budget through its own pool, or a
+// fixed-latency loop where a cudaMalloc (which may synchronise the device, and fails once
+// memory is exhausted) is not permitted.  For them one entry point takes its scratch from
+// this array, which the library image reserves on every GPU that loads it, until exit.
+// Host code must not use the array's name as a device address: the address is fetched per
+// device with cudaGetSymbolAddress.
+constexpr int64_t kNoAllocMaxN = VPM_NOALLOC_MAX_N;
+constexpr size_t kNoAllocScratchBytes = VPM_NOALLOC_SCRATCH_BYTES;
+constexpr size_t kNoAllocRecordBytes = size_t(kNoAllocMaxN) * 64;  // packed records
+static_assert(kNoAllocRecordBytes % kAlign == 0, "record region stays 256-byte aligned");
+static_assert(kNoAllocScratchBytes > kNoAllocRecordBytes, "room for partials");
+
+std::unordered_map<int, void*> g_noalloc_addr;  // device -> device address of the scratch
+
+int noalloc_scratch(void** out);
+
 // ---- FMA throughput kernels ------------------------------------------------------------
 template <class T>
 __global__ void fma_peak_kernel(int iters, T* sink) {
@@ -557,6 +577,29 @@ __global__ void fma_peak_kernel(int iters, T* sink) {
   sink[int64_t(blockIdx.x) * blockDim.x + threadIdx.x] = s;
 }
 
+}  // namespace
+
+// File-scope scratch of vpm_selfinduced_velocity_noalloc (see noalloc_scratch).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[VPM_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+// Device address of g_noalloc_scratch on the current device, looked up once per device
+// (with that device current) and cached.
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_noalloc_addr.find(dev);
+  if (it == g_noalloc_addr.end()) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-allocation scratch)");
+    it = g_noalloc_addr.emplace(dev, p).first;
+  }
+  *out = it->second;
+  return VPM_OK;
+}
 }  // namespace
 }  // namespace vpm
 
@@ -752,6 +795,34 @@ int vpm_sweep_records(int op, const void* records, int64_t n, int64_t target_beg
   c.records = records;
   c.tgt_begin = target_begin;
   if (n > 0 && !records) return fail(VPM_ERR_ARG, "null records pointer");
+  return dispatch(c, precision);
+}
+
+// Self-induced velocity without any allocation: the scratch (packed records and per-split
+// partial sums) lives in the library's static device array.  Every call shares that array
+// and leaves its contents behind; nothing in it needs clearing, because each call rewrites
+// every record and partial it reads.  Calls that overlap on the GPU (two streams, two host
+// threads) race on the array.  The first call on a device looks up the array's address
+// (cudaGetSymbolAddress) and the kernels' occupancy; make that first call before any stream
+// capture.
+int vpm_selfinduced_velocity_noalloc(const double* positions, const double* strengths,
+                                     const double* radii, int64_t n, double* velocities,
+                                     int precision, void* stream) {
+  if (n < 0) return fail(VPM_ERR_ARG, "negative size");
+  if (n > kNoAllocMaxN)
+    return fail(VPM_ERR_ARG, "n = " + std::to_string(n) +
+                                 " exceeds the no-allocation limit of " +
+                                 std::to_string(kNoAllocMaxN) +
+                                 " particles; call vpm_selfinduced_velocity with a workspace");
+  int rc = check_arch();
+  if (rc) return rc;
+  void* scratch = nullptr;
+  rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  Call c{VPM_OP_SELFINDUCED_VELOCITY, nullptr, n, positions, strengths, radii, nullptr, n,
+         velocities, nullptr, 0, scratch, kNoAllocScratchBytes,
+         static_cast<cudaStream_t>(stream)};
+  c.max_partial_bytes = kNoAllocScratchBytes - kNoAllocRecordBytes;
   return dispatch(c, precision);
 }
 
