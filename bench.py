@@ -396,8 +396,9 @@ def main():
         achieved = FLOPS_PER_PAIR_FUSED * pairs_per_launch / t_sweep / 1e12
         traffic = load_traffic()
         tr = None
-        if traffic and traffic.get("kernel_traffic_bytes_per_pair") is not None:
-            tr = traffic["kernel_traffic_bytes_per_pair"] * pairs_per_launch
+        if traffic and traffic.get("kernel_traffic_bytes_per_particle") is not None:
+            # DRAM traffic of the sweep grows with the particle count, not with N^2
+            tr = round(traffic["kernel_traffic_bytes_per_particle"] * n)
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms32, 3),
