@@ -147,6 +147,37 @@ int vpm_sweep_records(int op, const void* records, int64_t n, int64_t target_beg
                       int ref_extra_4pi, double* out, double* out2, int precision,
                       void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- device-resident time step (vpmModule.ParticleSystem), element-wise, HBM-bound ------ */
+/* out = x + c k over `count` doubles: RK stages (vpmModule.py:580,604,637,641,676,680,684). */
+int vpm_axpy(const double* x, const double* k, double c, int64_t count, double* out,
+             void* stream);
+/* out = x + dt/6 (k1 + 2 k2 + 2 k3 + k4): RK4 combine (vpmModule.py:688). */
+int vpm_rk4_combine(const double* x, const double* k1, const double* k2, const double* k3,
+                    const double* k4, double dt, int64_t count, double* out, void* stream);
+/* Strengths <- BDF ladder step `time_step` with rate coefficient `coef` (dt, 2/3 dt, 6/11 dt,
+ * 12/25 dt) and the reference's history rotation, in place (vpmModule.py:751-787, 801-841). */
+int vpm_bdf_update(double* strengths, double* hist1, double* hist2, double* hist3,
+                   const double* rate, int64_t count, int time_step, double coef, void* stream);
+/* sigma <- sqrt(sigma^2 + C (nu + nu_t) dt), in place (vpmModule.py:853-860). */
+int vpm_core_spreading(double* radii, const double* viscosities, const double* viscosities_t,
+                       int64_t n, double C, double dt, void* stream);
+/* Dynamic LES update (vpmModule.py:887-962): when advance_constant != 0, les_state =
+ * {Cnu, enstrophy_ref, initialised} (device doubles) is advanced with the device scalar
+ * `enstrophy` (vpmModule.py:887-909); then, for n > 0, nu_t is recomputed from the vorticity
+ * with the current Cnu and committed when its maximum exceeds 1e-9 (vpmModule.py:916-962;
+ * the maximum is written to nut_max when it is not NULL). */
+size_t vpm_les_workspace_bytes(int64_t n);
+int vpm_les_update(const double* vorticity, const double* radii, const double* enstrophy,
+                   int64_t n, int advance_constant, double* les_state, double* viscosities_t,
+                   double* nut_max, void* workspace, size_t workspace_bytes, void* stream);
+/* Strength relaxation towards the vorticity direction, in place (vpmModule.py:867-883). */
+int vpm_relax_strengths(double* strengths, const double* vorticity, int64_t n, double alpha,
+                        void* stream);
+/* FP64 O(N) diagnostics (vpmModule.py:264-284): out10 = [sum|a|, sum a (3),
+ * linear impulse 1/2 sum x x a (3), angular impulse 1/3 sum x x (x x a) (3)]. */
+int vpm_particle_diagnostics(const double* positions, const double* strengths, int64_t n,
+                             double* out10, void* stream);
+
 /* ---- no-allocation variant ------------------------------------------------------------ */
 #define VPM_NOALLOC_MAX_N 32768
 #define VPM_NOALLOC_SCRATCH_BYTES (8u << 20)

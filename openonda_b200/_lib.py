@@ -60,6 +60,14 @@ SIGNATURES = {
     "vpm_pack_records": ([_P, _P, _P, _P, _I64, _I, _P, _P], _I),
     "vpm_sweep_records": ([_I, _P, _I64, _I64, _I64, _I, _P, _P, _I, _P, _SZ, _P], _I),
     "vpm_selfinduced_velocity_noalloc": ([_P, _P, _P, _I64, _P, _I, _P], _I),
+    "vpm_axpy": ([_P, _P, ctypes.c_double, _I64, _P, _P], _I),
+    "vpm_rk4_combine": ([_P, _P, _P, _P, _P, ctypes.c_double, _I64, _P, _P], _I),
+    "vpm_bdf_update": ([_P, _P, _P, _P, _P, _I64, _I, ctypes.c_double, _P], _I),
+    "vpm_core_spreading": ([_P, _P, _P, _I64, ctypes.c_double, ctypes.c_double, _P], _I),
+    "vpm_les_workspace_bytes": ([_I64], _SZ),
+    "vpm_les_update": ([_P, _P, _P, _I64, _I, _P, _P, _P, _P, _SZ, _P], _I),
+    "vpm_relax_strengths": ([_P, _P, _I64, ctypes.c_double, _P], _I),
+    "vpm_particle_diagnostics": ([_P, _P, _I64, _P, _P], _I),
     "vpm_launch_fma_peak": ([_I, _I, _I, _I, _P, _P], _I),
 }
 

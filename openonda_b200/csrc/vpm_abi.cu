@@ -841,3 +841,6 @@ int vpm_launch_fma_peak(int fp64, int blocks, int threads, int iters, void* sink
 }
 
 }  // extern "C"
+
+// Element-wise time-step kernels and O(N) diagnostics (same translation unit).
+#include "vpm_step.cuh"

@@ -1,0 +1,756 @@
+"""Device-resident ``ParticleSystem`` with the interface of OpenONDA's vpmModule.
+
+Mirrors ``OpenONDA/solvers/VPM/vpmModule.py`` (class ``ParticleSystem``, :27-1121):
+same constructor keywords, same methods and the same time-step sequencing, but the particle
+state lives on the GPU as float64 tensors (positions/strengths/velocities ``(N,3)``,
+radii/viscosities ``(N,)``) instead of a Python list of ``Particle`` objects, and every
+step runs on the B200 library:
+
+* pair sums through :mod:`openonda_b200.kernels` (FP64 exact, or FP32-compensated with
+  ``precision="fp32c"``);
+* element-wise updates (RK stages and combine, BDF ladder with its history rotation, core
+  spreading, dynamic-LES constant and sub-grid viscosity, relaxation) and the O(N) FP64
+  diagnostics through the library's own kernels;
+* ``update_velocities`` evaluates velocity and stretching in one fused sweep when the flow
+  model needs stretching; ``update_strengths`` reuses that rate while the state is unchanged
+  (the reference evaluates both on the same positions/strengths, vpmModule.py:704,753-774).
+
+Reference behaviours kept: Euler/BDF2/BDF3/BDF4 ladder by ``time_step`` with the history
+rewritten after stretching and again after PSE; RK stage 1 reuses the velocities of
+``update_velocities``; "RK3" is the reference's midpoint variant; LES constant and psi test
+as in vpmModule.py:887-962; backup + diagnostics when ``time_step % backup_frequency == 0``.
+Deviation: ``relax_strength_solution`` normalises row-wise (the reference raises there,
+vpmModule.py:879), and ``subdivide_strong_particles`` uses the existing magnitude getter
+(the reference calls a missing method, :1065).
+
+Checkpoints: ``backup_particle_field`` writes the reference's VTP point cloud when pyvista is
+importable, and always an ``.npz`` with the same fields plus the BDF history, the LES state
+and the clock, so ``load_checkpoint`` resumes exactly.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import torch
+
+from .. import _lib, kernels
+
+EPSILON = 1e-9  # vpmModule.py:22
+CNU_0 = 0.02958  # vpmModule.py:92
+CORE_SPREADING_C = 5.34  # vpmModule.py:855
+RELAX_ALPHA = 0.95  # vpmModule.py:868
+
+_F64 = torch.float64
+
+
+class Particle:
+    """Host-side snapshot of one particle (OpenONDA/solvers/VPM/Particle.py:7-114)."""
+
+    def __init__(self, position=None, velocity=None, strength=None, radius=None, viscosity=None,
+                 viscosity_t=None, domain_size=1.0, group_id=0):
+        self.position = (np.array(position, dtype=np.float64) if position is not None
+                         else domain_size * np.random.random(3) - 1.0)
+        self.velocity = np.array(velocity if velocity is not None else np.zeros(3),
+                                 dtype=np.float64)
+        self.velocity_magnitude = np.linalg.norm(self.velocity)
+        self.strength = np.array(strength if strength is not None else np.zeros(3),
+                                 dtype=np.float64)
+        self.strength_magnitude = np.linalg.norm(self.strength)
+        self.radius = float(radius) if radius is not None else 0.01
+        self.viscosity = float(viscosity) if viscosity is not None else 0.0
+        self.viscosity_t = float(viscosity_t) if viscosity_t is not None else 0.0
+        self.viscosity_eff = self.viscosity + self.viscosity_t
+        self.group_id = group_id
+
+    def __str__(self):
+        p, v, s = self.position, self.velocity, self.strength
+        return (f"Location:({p[0]:.2E},{p[1]:.2E},{p[2]:.2E}) m, "
+                f"Velocity:({v[0]:.2E},{v[1]:.2E},{v[2]:.2E}) m/s, "
+                f"Strength:({s[0]:.2E},{s[1]:.2E},{s[2]:.2E}) m³/s, "
+                f"Radius: {self.radius:.2E} m, "
+                f"Viscosity: {self.viscosity:.2E} m²/s, "
+                f"Subgrid-scale viscosity: {self.viscosity_t:.2E} m²/s")
+
+
+def _stream(dev):
+    return torch.cuda.current_stream(dev).cuda_stream
+
+
+def _check(rc):
+    _lib.check(rc)
+
+
+class ParticleSystem:
+    """Particle system whose state and time step run on one B200."""
+
+    def __init__(self, time_step_size: float = 1.0, time_integration_method: str = "RK2",
+                 processing_unit: str = "GPU", flow_model: str = "DNS",
+                 viscous_scheme: str = "CoreSpreading", monitor_variables=None,
+                 flow_time: float = 0.0, time_step: int = 0, backup_frequency: int = 1,
+                 backup_filename: str = "particle_data", relax_strength_solution: bool = False,
+                 precision: str = "fp64", device=None, verbose: bool = False):
+        if monitor_variables is None:
+            monitor_variables = ["Circulation", "Linear Impulse", "Angular Impulse",
+                                 "Kinetic Energy", "Enstrophy", "Helicity"]
+        self._validate_float(time_step_size, "time_step_size")
+        self._validate_integration_method(time_integration_method)
+        self._validate_flow_model(flow_model)
+        self._validate_viscous_scheme(viscous_scheme)
+        self._validate_processing_unit(processing_unit)
+        _lib.precision_code(precision)
+
+        self.time_step_size = time_step_size
+        self.flow_time = flow_time
+        self.time_step = time_step
+        self.flow_model = flow_model
+        self.viscous_scheme = viscous_scheme
+        self.monitor_variables = monitor_variables
+        self.backup_filename = backup_filename
+        self.backup_frequency = backup_frequency
+        self.time_integration_method = time_integration_method
+        self.processing_unit = processing_unit
+        self.relax_strength_solution = relax_strength_solution
+        self.precision = precision
+        self.verbose = verbose
+        self.device = torch.device(device) if device is not None else None
+
+        if flow_model == "Potential":
+            self.flow_model_description = "Potential flow"
+            if viscous_scheme is not None:
+                raise ValueError("For 'Potential' flow model, 'viscous_scheme' must be None.")
+        elif flow_model == "pseudo2D":
+            self.flow_model_description = "(ν)(∇²)ω"
+            if viscous_scheme not in ["CoreSpreading", "PSE"]:
+                raise ValueError("For 'pseudo2D' flow model, 'viscous_scheme' must be "
+                                 "'CoreSpreading' or 'PSE'.")
+        elif flow_model == "LES":
+            self.flow_model_description = "(ω.∇)u + (ν+νt)(∇²)ω"
+            if viscous_scheme not in ["CoreSpreading", "PSE"]:
+                raise ValueError("For 'LES' flow model, 'viscous_scheme' must be "
+                                 "'CoreSpreading' or 'PSE'.")
+        elif flow_model == "DNS":
+            self.flow_model_description = "(ω.∇)u + (ν)(∇²)ω"
+            if viscous_scheme not in ["CoreSpreading", "PSE"]:
+                raise ValueError("For 'DNS' flow model, 'viscous_scheme' must be "
+                                 "'CoreSpreading' or 'PSE'.")
+
+        self._n = 0
+        self._x = self._a = self._u = None
+        self._s = self._nu = self._nut = None
+        self._gid = np.zeros(0, dtype=np.int64)
+        self._hist = None
+        self._les = None  # device [Cnu, enstrophy_ref, initialised]
+        self._cnu_host = CNU_0
+        self._rate = None  # stretching rate from the fused sweep, valid for self._rate_token
+        self._rate_token = None
+        self._token = 0
+
+    # ---- validation (vpmModule.py:158-184) ------------------------------------------
+    def _validate_float(self, value, name):
+        if not isinstance(value, (float, int, np.float64)):
+            raise TypeError(f"{name} must be a float or int, got {type(value).__name__}")
+
+    def _validate_integration_method(self, method):
+        valid = {"Euler", "RK2", "RK3", "RK4"}
+        if method not in valid:
+            raise ValueError(f"Invalid time integration method '{method}'. Choose from {valid}.")
+
+    def _validate_viscous_scheme(self, scheme):
+        valid = {"PSE", "CoreSpreading", None}
+        if scheme not in valid:
+            raise ValueError(f"Invalid viscous scheme '{scheme}'. Choose from {valid}.")
+
+    def _validate_processing_unit(self, unit):
+        valid = {"GPU", "B200"}
+        if unit not in valid:
+            raise ValueError(f"Invalid processing unit '{unit}'. This ParticleSystem runs on "
+                             f"the B200; choose from {valid}.")
+
+    def _validate_flow_model(self, method):
+        valid = {"Potential", "pseudo2D", "DNS", "LES"}
+        if method not in valid:
+            raise ValueError(f"Invalid time integration method '{method}'. Choose from {valid}.")
+
+    # ---- device state ------------------------------------------------------------------
+    def _dev(self):
+        if self.device is None:
+            if not torch.cuda.is_available():
+                raise RuntimeError("ParticleSystem needs a CUDA device (B200); none is visible")
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        return self.device
+
+    def _touch(self):
+        self._token += 1
+
+    def _les_state(self):
+        if self._les is None:
+            self._les = torch.tensor([self._cnu_host, 0.0, 0.0], dtype=_F64, device=self._dev())
+        return self._les
+
+    @property
+    def Cnu(self) -> float:
+        return float(self._les[0]) if self._les is not None else self._cnu_host
+
+    @Cnu.setter
+    def Cnu(self, value):
+        self._cnu_host = float(value)
+        if self._les is not None:
+            self._les[0] = float(value)
+
+    @property
+    def enstrophy_ref(self):
+        if self._les is None or float(self._les[2]) == 0.0:
+            return None
+        return float(self._les[1])
+
+    # ---- system information -------------------------------------------------------------
+    def __len__(self):
+        return self._n
+
+    def __getitem__(self, index):
+        return self._particle(index)
+
+    def __iter__(self):
+        return (self._particle(i) for i in range(self._n))
+
+    def _particle(self, i):
+        if i < 0:
+            i += self._n
+        if not 0 <= i < self._n:
+            raise IndexError("particle index out of range")
+        return Particle(position=self._x[i].cpu().numpy(), velocity=self._u[i].cpu().numpy(),
+                        strength=self._a[i].cpu().numpy(), radius=float(self._s[i]),
+                        viscosity=float(self._nu[i]), viscosity_t=float(self._nut[i]),
+                        group_id=int(self._gid[i]))
+
+    def __str__(self):
+        return (
+            f"\n{'=' * 60}\n"
+            f"Particle System with {self._n} particles\n"
+            f"{'-' * 60}\n"
+            f"Starting from step:  {self.time_step}\n"
+            f"Simulation Time:     {self.flow_time:.3E} s\n"
+            f"Time Step Size:      {self.time_step_size:.3E} s\n"
+            f"Viscous scheme:      {self.viscous_scheme}\n"
+            f"Total strength:      {self.get_total_strength_magnitude():.3E} m³/s\n"
+            f"Integration Method:  {self.time_integration_method}\n"
+            f"Processing Unit:     {self.processing_unit}\n"
+            f"Precision:           {self.precision}\n"
+            f"Flow Model:          {self.flow_model}\n"
+            f"Monitor Variables:   {', '.join(self.monitor_variables)}\n"
+            f"Backup Frequency:    Every {self.backup_frequency} time steps\n"
+            f"Backup Filename:     {self.backup_filename}\n"
+            f"{'=' * 60}"
+        )
+
+    def _log(self, msg):
+        if self.verbose:
+            print(msg)
+
+    # ---- getters (numpy copies, like vpmModule.py:219-251) ---------------------------
+    def _np(self, t, shape):
+        return np.zeros(shape) if t is None else t.cpu().numpy()
+
+    def get_particle_positions(self):
+        return self._np(self._x, (0, 3))
+
+    def get_particle_group_id(self):
+        return self._gid.copy()
+
+    def get_particle_strengths(self):
+        return self._np(self._a, (0, 3))
+
+    def get_particle_velocities(self):
+        return self._np(self._u, (0, 3))
+
+    def get_particle_radii(self):
+        return self._np(self._s, (0,))
+
+    def get_particle_viscosities(self):
+        return self._np(self._nu, (0,))
+
+    def get_particle_viscosities_t(self):
+        return self._np(self._nut, (0,))
+
+    def get_particle_viscosities_eff(self):
+        return self._np(None if self._nu is None else self._nu + self._nut, (0,))
+
+    def get_particle_strength_magnitudes(self) -> np.ndarray:
+        if self._a is None:
+            return np.zeros(0)
+        return torch.linalg.vector_norm(self._a, dim=1).cpu().numpy()
+
+    # device views for tensor users
+    @property
+    def positions(self):
+        return self._x
+
+    @property
+    def strengths(self):
+        return self._a
+
+    @property
+    def radii(self):
+        return self._s
+
+    @property
+    def velocities(self):
+        return self._u
+
+    # ---- pair sums -----------------------------------------------------------------------
+    def get_particle_vorticities(self) -> np.ndarray:
+        return self._vorticity().cpu().numpy()
+
+    def _vorticity(self):
+        return kernels.vorticity_field_at(self._x, self._x, self._a, self._s,
+                                          precision=self.precision)
+
+    def _diagnostics(self):
+        out = torch.empty(10, dtype=_F64, device=self._dev())
+        _check(_lib.load().vpm_particle_diagnostics(
+            self._x.data_ptr() if self._n else None, self._a.data_ptr() if self._n else None,
+            self._n, out.data_ptr(), _stream(self._dev())))
+        return out.cpu().numpy()
+
+    def get_total_linear_impulse(self) -> np.ndarray:
+        return self._diagnostics()[4:7]
+
+    def get_total_angular_impulse(self) -> np.ndarray:
+        return self._diagnostics()[7:10]
+
+    def get_total_strength(self):
+        return self._diagnostics()[1:4]
+
+    def get_total_strength_magnitude(self) -> float:
+        if self._n == 0:
+            return 0.0
+        return float(self._diagnostics()[0])
+
+    def get_total_enstrophy(self) -> float:
+        return float(kernels.total_enstrophy(self._x, self._a, self._s, ref_extra_4pi=True,
+                                             precision="fp64"))
+
+    def get_total_kinetic_energy(self) -> float:
+        return float(kernels.total_kinetic_energy(self._x, self._a, self._s, precision="fp64"))
+
+    def get_total_helicity(self) -> float:
+        return float(kernels.total_helicity(self._x, self._a, self._s, ref_extra_4pi=True,
+                                            precision="fp64"))
+
+    def _as_dev(self, arr):
+        if isinstance(arr, torch.Tensor):
+            return arr.to(device=self._dev(), dtype=_F64).contiguous()
+        return torch.from_numpy(np.ascontiguousarray(np.asarray(arr, dtype=np.float64))).to(
+            self._dev())
+
+    def get_vorticity_field_at(self, grid_positions):
+        t = self._as_dev(grid_positions)
+        return kernels.vorticity_field_at(t, self._x, self._a, self._s,
+                                          precision=self.precision).cpu().numpy()
+
+    def get_induced_velocity_at(self, grid_positions):
+        t = self._as_dev(grid_positions)
+        return kernels.induced_velocity_at(t, self._x, self._a, self._s,
+                                           precision=self.precision).cpu().numpy()
+
+    # ---- diagnostics (vpmModule.py:351-383) --------------------------------------------
+    def log_diagnostics(self):
+        print("\n" + "=" * 60)
+        print(f"{'Flow Diagnostics':^5}")
+        print("-" * 60)
+        print(f"Flow time: {self.flow_time:0.3E} s")
+        print(f"Time step: {self.time_step}\n")
+        mv = self.monitor_variables
+        if "Circulation" in mv:
+            print(f"{'Circulation':<20}: {self.get_total_strength_magnitude():0.3E} m³/s")
+        if "Kinetic energy" in mv:
+            print(f"{'Kinetic energy':<20}: {self.get_total_kinetic_energy():0.3E} m⁵/s²")
+        if "Linear impulse" in mv:
+            i = self.get_total_linear_impulse()
+            print(f"{'Linear Impulse':<20}: ({i[0]:0.3E}, {i[1]:0.3E}, {i[2]:0.3E}) m⁴/s")
+        if "Angular impulse" in mv:
+            a = self.get_total_angular_impulse()
+            print(f"{'Angular Impulse':<20}: ({a[0]:0.3E}, {a[1]:0.3E}, {a[2]:0.3E}) m⁵/s")
+        if "Enstrophy" in mv:
+            print(f"{'Total enstrophy':<20}: {self.get_total_enstrophy():0.3E} m³/s²")
+        if "Helicity" in mv:
+            print(f"{'Total helicity':<20}: {self.get_total_helicity():0.3E} m²/s²")
+        print("=" * 60 + "\n")
+
+    # ---- particle initialisation and management ---------------------------------------
+    def add_particle(self, particle: Particle):
+        self._append(np.asarray(particle.position, np.float64)[None],
+                     np.asarray(particle.velocity, np.float64)[None],
+                     np.asarray(particle.strength, np.float64)[None],
+                     np.array([particle.radius], np.float64),
+                     np.array([particle.viscosity], np.float64),
+                     np.array([particle.viscosity_t], np.float64),
+                     np.array([particle.group_id], np.int64))
+
+    def add_particle_field(self, positions, velocities, strengths, radii, viscosities,
+                           viscosities_t=None, group_id=None):
+        positions, velocities, strengths = (np.asarray(z) for z in (positions, velocities,
+                                                                   strengths))
+        radii, viscosities = np.asarray(radii), np.asarray(viscosities)
+        n = positions.shape[0]
+        if positions.shape[1] != 3 or velocities.shape[1] != 3 or strengths.shape[1] != 3:
+            raise ValueError("Positions, velocities, and strengths must be of shape (N x 3).")
+        if radii.shape[0] != n or viscosities.shape[0] != n:
+            raise ValueError("Radii and viscosities must have the same number of elements as "
+                             "positions.")
+        if viscosities_t is None:
+            viscosities_t = np.zeros_like(viscosities, dtype=np.float64)
+        if group_id is None:
+            group_id = np.zeros(n, dtype=np.int64)
+        elif isinstance(group_id, int):
+            group_id = np.full(n, group_id, dtype=np.int64)
+        self._append(positions, velocities, strengths, radii, viscosities,
+                     np.asarray(viscosities_t), np.asarray(group_id, dtype=np.int64))
+
+    def _append(self, x, u, a, s, nu, nut, gid):
+        dev = self._dev()
+        t = lambda z: torch.as_tensor(np.ascontiguousarray(np.asarray(z, np.float64)), device=dev)
+        if self._n == 0:
+            self._x, self._u, self._a = t(x).reshape(-1, 3), t(u).reshape(-1, 3), \
+                t(a).reshape(-1, 3)
+            self._s, self._nu, self._nut = t(s).reshape(-1), t(nu).reshape(-1), \
+                t(nut).reshape(-1)
+            self._gid = np.asarray(gid, np.int64).reshape(-1).copy()
+        else:
+            self._x = torch.cat([self._x, t(x).reshape(-1, 3)])
+            self._u = torch.cat([self._u, t(u).reshape(-1, 3)])
+            self._a = torch.cat([self._a, t(a).reshape(-1, 3)])
+            self._s = torch.cat([self._s, t(s).reshape(-1)])
+            self._nu = torch.cat([self._nu, t(nu).reshape(-1)])
+            self._nut = torch.cat([self._nut, t(nut).reshape(-1)])
+            self._gid = np.concatenate([self._gid, np.asarray(gid, np.int64).reshape(-1)])
+        self._n = int(self._x.shape[0])
+        self._hist = None if self._hist is None else self._resize_hist()
+        self._touch()
+
+    def _resize_hist(self):
+        n = self._n
+        out = []
+        for h in self._hist:
+            if h.shape[0] < n:
+                h = torch.cat([h, torch.zeros((n - h.shape[0], 3), dtype=_F64,
+                                              device=h.device)])
+            out.append(h[:n].contiguous())
+        return out
+
+    def _keep(self, mask):
+        if self._n == 0:
+            return
+        m = torch.as_tensor(mask, device=self._dev())
+        self._x, self._u, self._a = self._x[m], self._u[m], self._a[m]
+        self._s, self._nu, self._nut = self._s[m], self._nu[m], self._nut[m]
+        self._gid = self._gid[np.asarray(mask)]
+        if self._hist is not None:
+            self._hist = [h[m].contiguous() for h in self._hist]
+        self._n = int(self._x.shape[0])
+        self._touch()
+
+    def remove_particles(self, particle_indices: list):
+        keep = np.ones(self._n, dtype=bool)
+        for index in set(int(i) for i in particle_indices):
+            if 0 <= index < self._n:
+                keep[index] = False
+        self._keep(keep)
+        self._log(f"(info) Removed {len(particle_indices)} particles")
+
+    def remove_all_particles(self):
+        self._keep(np.zeros(self._n, dtype=bool))
+        self._log("(info) Removed all particles from particle system.")
+
+    def print_particle_information(self, index=None):
+        print("\nParticle system information ({} particles):".format(len(self)))
+        if index is None:
+            for p in self:
+                print(p)
+        elif isinstance(index, int):
+            print(self[index])
+
+    # ---- checkpoint / backup (vpmModule.py:466-516) -------------------------------------
+    def _backup_name(self, ext):
+        return f"{self.backup_filename}_{str(self.time_step).zfill(7)}.{ext}"
+
+    def backup_particle_field(self):
+        """Write the reference's VTP point cloud (when pyvista is importable) and an .npz
+        checkpoint holding the same fields plus the state needed to resume exactly."""
+        try:
+            import pyvista as pv  # optional, as in the reference
+        except ImportError:
+            pv = None
+        if pv is not None and hasattr(pv, "PolyData"):
+            cloud = pv.PolyData(self.get_particle_positions())
+            cloud.point_data["Velocity"] = self.get_particle_velocities()
+            cloud.point_data["Strength"] = self.get_particle_strengths()
+            cloud.point_data["Radius"] = self.get_particle_radii()
+            cloud.point_data["Group_ID"] = self.get_particle_group_id()
+            cloud.point_data["Viscosity"] = self.get_particle_viscosities()
+            cloud.point_data["Viscosity_t"] = self.get_particle_viscosities_t()
+            cloud.save(self._backup_name("vtp"))
+        self.save_checkpoint(self._backup_name("npz"))
+
+    def save_checkpoint(self, filename):
+        d = dict(Position=self.get_particle_positions(), Velocity=self.get_particle_velocities(),
+                 Strength=self.get_particle_strengths(), Radius=self.get_particle_radii(),
+                 Group_ID=self.get_particle_group_id(), Viscosity=self.get_particle_viscosities(),
+                 Viscosity_t=self.get_particle_viscosities_t(),
+                 time_step=np.int64(self.time_step), flow_time=np.float64(self.flow_time),
+                 time_step_size=np.float64(self.time_step_size))
+        if self._hist is not None:
+            for k, h in enumerate(self._hist):
+                d[f"history_{k + 1}"] = h.cpu().numpy()
+        if self._les is not None:
+            d["les_state"] = self._les.cpu().numpy()
+        else:
+            d["les_state"] = np.array([self._cnu_host, 0.0, 0.0])
+        os.makedirs(os.path.dirname(os.path.abspath(filename)) or ".", exist_ok=True)
+        np.savez(filename, **d)
+
+    def load_checkpoint(self, filename):
+        """Restore the full state written by save_checkpoint (exact resume)."""
+        d = np.load(filename)
+        self.remove_all_particles()
+        self.add_particle_field(d["Position"], d["Velocity"], d["Strength"], d["Radius"],
+                                d["Viscosity"], d["Viscosity_t"], d["Group_ID"])
+        self.time_step = int(d["time_step"])
+        self.flow_time = float(d["flow_time"])
+        if "history_1" in d.files:
+            self._hist = [self._as_dev(d[f"history_{k}"]) for k in (1, 2, 3)]
+        self._les = self._as_dev(d["les_state"])
+        self._cnu_host = float(d["les_state"][0])
+
+    def load_particle_field_from_backup(self, filename: str):
+        """Load a VTP backup (needs pyvista) or an .npz checkpoint."""
+        if filename.endswith(".npz"):
+            d = np.load(filename)
+            self.add_particle_field(d["Position"], d["Velocity"], d["Strength"], d["Radius"],
+                                    d["Viscosity"], d["Viscosity_t"], d["Group_ID"])
+            return
+        import pyvista as pv
+
+        cloud = pv.read(filename)
+        self.add_particle_field(np.array(cloud.points, dtype=np.float64),
+                                np.array(cloud.point_data["Velocity"], dtype=np.float64),
+                                np.array(cloud.point_data["Strength"], dtype=np.float64),
+                                np.array(cloud.point_data["Radius"], dtype=np.float64),
+                                np.array(cloud.point_data["Viscosity"], dtype=np.float64),
+                                np.array(cloud.point_data["Viscosity_t"], dtype=np.float64),
+                                np.array(cloud.point_data["Group_ID"], dtype=np.int64))
+
+    # ---- time integration (vpmModule.py:522-692) ---------------------------------------
+    def update_dt(self, time_step_size: float):
+        self.time_step_size = time_step_size
+
+    def _vel(self, x):
+        return kernels.selfinduced_velocity(x, self._a, self._s, precision=self.precision)
+
+    def _axpy(self, x, k, c):
+        out = torch.empty_like(x)
+        _check(_lib.load().vpm_axpy(x.data_ptr(), k.data_ptr(), float(c), x.numel(),
+                                    out.data_ptr(), _stream(self._dev())))
+        return out
+
+    def update_state(self):
+        """Advance positions with the chosen integrator, back up and log at the backup
+        frequency, then advance the clock (vpmModule.py:522-560)."""
+        self.time_integration_method = self.time_integration_method.strip()
+        methods = {"Euler": self._euler_update_position, "RK2": self._rk2_update_position,
+                   "RK3": self._rk3_update_position, "RK4": self._rk4_update_position}
+        if self.time_integration_method not in methods:
+            raise ValueError(f"Unknown time integration method: {self.time_integration_method}")
+        new_x = methods[self.time_integration_method](self._x, self._u) if self._n else self._x
+        if self.time_step % self.backup_frequency == 0:
+            self.backup_particle_field()
+            if self.monitor_variables:
+                self.log_diagnostics()
+        self.flow_time += self.time_step_size
+        self.time_step += 1
+        self._x = new_x
+        self._touch()
+
+    def _euler_update_position(self, positions, velocities_1):
+        return self._axpy(positions, velocities_1, self.time_step_size)
+
+    def _rk2_update_position(self, positions, velocities_1):
+        dt = self.time_step_size
+        k2 = self._vel(self._axpy(positions, velocities_1, dt * 0.5))
+        return self._axpy(positions, k2, dt)
+
+    def _rk3_update_position(self, positions, velocities_1):
+        dt = self.time_step_size
+        k2 = self._vel(self._axpy(positions, velocities_1, dt / 2))
+        k3 = self._vel(self._axpy(positions, k2, dt / 2))
+        return self._axpy(positions, k3, dt)
+
+    def _rk4_update_position(self, positions, velocities_1):
+        dt = self.time_step_size
+        k1 = velocities_1
+        k2 = self._vel(self._axpy(positions, k1, dt / 2))
+        k3 = self._vel(self._axpy(positions, k2, dt / 2))
+        k4 = self._vel(self._axpy(positions, k3, dt))
+        out = torch.empty_like(positions)
+        _check(_lib.load().vpm_rk4_combine(positions.data_ptr(), k1.data_ptr(), k2.data_ptr(),
+                                           k3.data_ptr(), k4.data_ptr(), float(dt),
+                                           positions.numel(), out.data_ptr(),
+                                           _stream(self._dev())))
+        return out
+
+    def update_velocities(self):
+        """Self-induced velocities (vpmModule.py:699-710); with stretching in the flow model
+        the same sweep also yields the stretching rate for update_strengths."""
+        if self._n == 0:
+            return
+        if self.flow_model in ("LES", "DNS"):
+            self._u, self._rate = kernels.velocity_and_strength_gradients(
+                self._x, self._a, self._s, precision=self.precision)
+            self._rate_token = self._token
+        else:
+            self._u = self._vel(self._x)
+        self._log("• Updated particles' velocities")
+
+    def _stretching_rate(self):
+        if self._rate is not None and self._rate_token == self._token:
+            return self._rate
+        return kernels.strength_gradients(self._x, self._a, self._s, precision=self.precision)
+
+    def _bdf(self, rate):
+        if self._hist is None:
+            self._hist = [torch.zeros_like(self._a) for _ in range(3)]
+        dt, k = self.time_step_size, self.time_step
+        coef = {0: dt, 1: (2 / 3) * dt, 2: (6 / 11) * dt}.get(k, (12 / 25) * dt)
+        h1, h2, h3 = self._hist
+        _check(_lib.load().vpm_bdf_update(self._a.data_ptr(), h1.data_ptr(), h2.data_ptr(),
+                                          h3.data_ptr(), rate.data_ptr(), self._a.numel(),
+                                          int(k), float(coef), _stream(self._dev())))
+
+    def update_strengths(self):
+        """Strength update (vpmModule.py:713-884): LES filter update, stretching (BDF ladder),
+        PSE (BDF ladder on the post-stretching strengths) or core spreading, relaxation."""
+        if self.flow_model == "Potential":
+            self._log("• Update_strengths() ignored because flow model is set to potential "
+                      "flow.")
+            return
+        if self._n == 0:
+            return
+        dev = self._dev()
+        if self.flow_model == "LES":
+            w = self._vorticity()
+            ens = kernels.total_enstrophy(self._x, self._a, self._s, ref_extra_4pi=True,
+                                          precision=self.precision)
+            self._les_update(w, ens)
+        rate_s = None
+        if self.flow_model in ("LES", "DNS"):
+            rate_s = self._stretching_rate()
+        if self._hist is None:
+            self._hist = [torch.zeros_like(self._a) for _ in range(3)]
+        if rate_s is not None:
+            self._bdf(rate_s)
+            self._touch()
+        if self.viscous_scheme == "PSE":
+            nu_eff = self._nu + self._nut
+            rate_p = kernels.strength_gradients_pse(self._x, self._a, self._s, nu_eff,
+                                                    precision=self.precision)
+            self._bdf(rate_p)
+            self._touch()
+        elif self.viscous_scheme == "CoreSpreading":
+            _check(_lib.load().vpm_core_spreading(
+                self._s.data_ptr(), self._nu.data_ptr(), self._nut.data_ptr(), self._n,
+                CORE_SPREADING_C, float(self.time_step_size), _stream(dev)))
+            self._touch()
+        if self.relax_strength_solution:
+            w = self._vorticity()
+            _check(_lib.load().vpm_relax_strengths(self._a.data_ptr(), w.data_ptr(), self._n,
+                                                   RELAX_ALPHA, _stream(dev)))
+            self._touch()
+
+    def _les_update(self, vorticity, enstrophy, advance_constant=True):
+        dev = self._dev()
+        st = self._les_state()
+        lib = _lib.load()
+        nb = lib.vpm_les_workspace_bytes(self._n)
+        ws = torch.empty(max(nb, 256), dtype=torch.uint8, device=dev)
+        nut_max = torch.empty((), dtype=_F64, device=dev)
+        _check(lib.vpm_les_update(
+            vorticity.data_ptr(), self._s.data_ptr(),
+            None if enstrophy is None else enstrophy.data_ptr(), self._n,
+            int(advance_constant), st.data_ptr(), self._nut.data_ptr(), nut_max.data_ptr(),
+            ws.data_ptr(), ws.numel(), _stream(dev)))
+        self._nut_max = nut_max
+
+    def _update_LES_filter_constant(self, enstrophy: float):
+        """Dynamic constant update from an enstrophy value (vpmModule.py:887-909)."""
+        e = torch.tensor(float(enstrophy), dtype=_F64, device=self._dev())
+        _check(_lib.load().vpm_les_update(None, None, e.data_ptr(), 0, 1,
+                                          self._les_state().data_ptr(), None, None, None, 0,
+                                          _stream(self._dev())))
+
+    def _update_LES_particles_viscosity(self, vorticity, radii):
+        """Sub-grid viscosity from a vorticity field with the current Cnu
+        (vpmModule.py:916-962); `radii` are the particles' own (kept for the signature)."""
+        self._les_update(self._as_dev(vorticity), None, advance_constant=False)
+
+    # ---- particle field control (vpmModule.py:970-1121) --------------------------------
+    def remove_weak_particles(self, mode: str, threshold: float, conserve_total_circulation=False):
+        mags = self.get_particle_strength_magnitudes()
+        total_before = np.sum(mags)
+        if len(mags) == 0:
+            print("(warning) No particles available to evaluate.")
+            return
+        if mode == "absolute":
+            weak = mags < threshold
+        elif mode == "relative":
+            highest = np.max(mags)
+            if highest == 0:
+                print("(warning) All particle strengths are zero.")
+                weak = np.ones_like(mags, dtype=bool)
+            else:
+                weak = mags / highest < threshold
+        else:
+            print(f"(error) Mode '{mode}' not recognized. Use 'absolute' or 'relative'.")
+            return
+        self.remove_particles(np.where(weak)[0])
+        if conserve_total_circulation and self._n:
+            total_after = np.sum(self.get_particle_strength_magnitudes())
+            self._a = self._a * (total_before / total_after)
+            self._touch()
+
+    def subdivide_strong_particles(self, top_percentage=None, strength_threshold=None):
+        if top_percentage is None and strength_threshold is None:
+            raise ValueError("Provide either top_percentage or strength_threshold.")
+        mags = self.get_particle_strength_magnitudes()
+        idx = get_highest_nonzero_indices(mags, top_percentage=top_percentage,
+                                          strength_threshold=strength_threshold)
+        x, a, s = self.get_particle_positions(), self.get_particle_strengths(), \
+            self.get_particle_radii()
+        for p in idx:
+            half = a[p] / 2
+            dx = s[p] * a[p] / mags[p]
+            for sign in (1.0, -1.0):
+                self.add_particle(Particle(position=x[p] + sign * dx * 0.25,
+                                           velocity=np.zeros(3), strength=half))
+        self.remove_particles(list(idx))
+
+    def remesh_solution(self, flow2D: bool = False):
+        """The reference's remesh (vpmModule.py:1097-1121) builds a grid and stops before
+        changing the particles; it leaves the state unchanged, and so does this one."""
+        return None
+
+
+def get_highest_nonzero_indices(arr, top_percentage=None, strength_threshold=None):
+    """Indices of the highest non-zero entries (vpmModule.py:1124-1166)."""
+    arr = np.asarray(arr)
+    nz = np.nonzero(arr)[0]
+    vals = arr[nz]
+    order = np.argsort(vals)[::-1]
+    if top_percentage is not None:
+        top_n = max(int(top_percentage * len(nz) / 100), 1)
+        return nz[order[:top_n]]
+    if strength_threshold is not None:
+        ok = vals > strength_threshold
+        vals, nz = vals[ok], nz[ok]
+        order = np.argsort(vals)[::-1]
+    return nz[order]
