@@ -53,7 +53,10 @@ enum vpm_op {
   VPM_OP_TOTAL_KINETIC_ENERGY = 5,
   VPM_OP_TOTAL_HELICITY = 6,
   VPM_OP_TOTAL_ENSTROPHY = 7,
-  VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS = 8
+  VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS = 8,
+  VPM_OP_RHS_VJP = 9,             /* adjoint of (velocity, stretching) */
+  VPM_OP_RHS_VJP_PSE = 10,        /* adjoint of (velocity, stretching + PSE) */
+  VPM_OP_KINETIC_ENERGY_GRAD = 11 /* gradient of the kinetic energy */
 };
 
 /* ---- library information ------------------------------------------------------------ */
@@ -129,6 +132,25 @@ int vpm_velocity_and_strength_gradients(const double* positions, const double* s
                                         const double* radii, int64_t n, double* velocities,
                                         double* dalpha_dt, int precision, void* workspace,
                                         size_t workspace_bytes, void* stream);
+
+/* ---- adjoint (differentiation form; no counterpart in the reference) ------------------ */
+/* Vector-Jacobian product of the right-hand side F = (u, S [+ P]) of the coupled ODE
+ * dx/dt = u, dalpha/dt = S + P, where u, S, P are the sums of vpm_selfinduced_velocity,
+ * vpm_strength_gradients and vpm_strength_gradients_pse: given cotangents grad_velocities
+ * and grad_rates (n,3), writes (dL/dx, dL/dalpha) (n,3), dL/dsigma (n,) and, when
+ * `viscosities` is not NULL (PSE included), dL/dnu (n,) into grad_viscosities (may be NULL).
+ * One deterministic sweep over all pairs; workspace from vpm_workspace_bytes(VPM_OP_RHS_VJP
+ * or VPM_OP_RHS_VJP_PSE, precision, n, n). */
+int vpm_rhs_vjp(const double* positions, const double* strengths, const double* radii,
+                const double* viscosities, int64_t n, const double* grad_velocities,
+                const double* grad_rates, double* grad_positions, double* grad_strengths,
+                double* grad_radii, double* grad_viscosities, int precision, void* workspace,
+                size_t workspace_bytes, void* stream);
+/* Gradient of vpm_total_kinetic_energy w.r.t. positions, strengths and radii. */
+int vpm_kinetic_energy_grad(const double* positions, const double* strengths,
+                            const double* radii, int64_t n, double* grad_positions,
+                            double* grad_strengths, double* grad_radii, int precision,
+                            void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- pre-packed records (device-resident state, target shards) ----------------------- */
 /* Bytes of one packed particle record (64; FP32 records hold every value twice). */

@@ -31,6 +31,9 @@ OPS = {
     "total_helicity": 6,
     "total_enstrophy": 7,
     "velocity_and_strength_gradients": 8,
+    "rhs_vjp": 9,
+    "rhs_vjp_pse": 10,
+    "kinetic_energy_grad": 11,
 }
 
 _P = ctypes.c_void_p
@@ -56,6 +59,8 @@ SIGNATURES = {
     "vpm_total_helicity": ([_P, _P, _P, _I64, _I, _P, _I, _P, _SZ, _P], _I),
     "vpm_total_enstrophy": ([_P, _P, _P, _I64, _I, _P, _I, _P, _SZ, _P], _I),
     "vpm_velocity_and_strength_gradients": ([_P, _P, _P, _I64, _P, _P, _I, _P, _SZ, _P], _I),
+    "vpm_rhs_vjp": ([_P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _I, _P, _SZ, _P], _I),
+    "vpm_kinetic_energy_grad": ([_P, _P, _P, _I64, _P, _P, _P, _I, _P, _SZ, _P], _I),
     "vpm_record_bytes": ([_I], _SZ),
     "vpm_pack_records": ([_P, _P, _P, _P, _I64, _I, _P, _P], _I),
     "vpm_sweep_records": ([_I, _P, _I64, _I64, _I64, _I, _P, _P, _I, _P, _SZ, _P], _I),

@@ -16,6 +16,7 @@
 
 #include "vpm_b200.h"
 #include "vpm_sweep.cuh"
+#include "vpm_adjoint.cuh"
 
 namespace vpm {
 namespace {
@@ -106,10 +107,15 @@ int check_arch() {
 template <class Op, class T>
 struct Sweep {
   using C = Cfg<T>;
+  using RecT = typename Op::Record;
   static constexpr int NV = Op::NV;
-  static constexpr size_t kSmem = sweep_smem_bytes<T, Op::NV, C::R, C::THREADS, C::TILE, C::STAGES>();
+  static constexpr int R = Op::kR ? Op::kR : C::R;
+  // the same tile bytes for every record width
+  static constexpr int TILE = int(C::TILE * sizeof(Rec<T>) / sizeof(RecT));
+  static constexpr size_t kSmem =
+      sweep_smem_bytes<T, RecT, Op::NV, R, C::THREADS, TILE, C::STAGES>();
   static void* kernel() {
-    return reinterpret_cast<void*>(&sweep_kernel<Op, T, C::R, C::THREADS, C::TILE, C::STAGES>);
+    return reinterpret_cast<void*>(&sweep_kernel<Op, T, R, C::THREADS, TILE, C::STAGES>);
   }
 
   static int plan(int64_t m, int64_t n, Plan* p, size_t max_partial_bytes = kMaxPartialBytes) {
@@ -138,11 +144,11 @@ struct Sweep {
       }
     }
     if (occ < 1) occ = 1;
-    const int64_t per_block = int64_t(C::THREADS) * C::R;
+    const int64_t per_block = int64_t(C::THREADS) * R;
     p->tblocks = (m + per_block - 1) / per_block;
     p->smem = kSmem;
     p->threads = C::THREADS;
-    p->r = C::R;
+    p->r = R;
     p->nv = NV;
     p->splits = 1;
     p->chunk = n;
@@ -172,11 +178,11 @@ struct Sweep {
     return size_t(p.splits) * NV * size_t(m) * sizeof(double);
   }
 
-  static int launch(const Plan& p, const Rec<T>* tgt, int64_t m, int64_t tgt_offset,
-                    const Rec<T>* src, int64_t n, double* partial, cudaStream_t st) {
-    SweepArgs<T> a{tgt, m, tgt_offset, src, n, p.chunk, partial};
+  static int launch(const Plan& p, const RecT* tgt, int64_t m, int64_t tgt_offset,
+                    const RecT* src, int64_t n, double* partial, cudaStream_t st) {
+    SweepArgs<RecT> a{tgt, m, tgt_offset, src, n, p.chunk, partial};
     dim3 grid(unsigned(p.tblocks), unsigned(p.splits));
-    sweep_kernel<Op, T, C::R, C::THREADS, C::TILE, C::STAGES><<<grid, C::THREADS, p.smem, st>>>(a);
+    sweep_kernel<Op, T, R, C::THREADS, TILE, C::STAGES><<<grid, C::THREADS, p.smem, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
     return VPM_OK;
@@ -325,6 +331,87 @@ int zero_out(double* p, int64_t count, cudaStream_t st) {
   return VPM_OK;
 }
 
+// ---- adjoint: pack, finalize --------------------------------------------------------------
+template <class E>
+__global__ void pack_grad_kernel(const double* __restrict__ pos, const double* __restrict__ str,
+                                 const double* __restrict__ rad, const double* __restrict__ nu,
+                                 const double* __restrict__ gu, const double* __restrict__ gs,
+                                 int64_t n, RecG<E>* __restrict__ out) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  RecG<E> r;
+  set_elem(r.x, pos[3 * i]);
+  set_elem(r.y, pos[3 * i + 1]);
+  set_elem(r.z, pos[3 * i + 2]);
+  set_elem(r.s, rad[i]);
+  set_elem(r.ax, str[3 * i]);
+  set_elem(r.ay, str[3 * i + 1]);
+  set_elem(r.az, str[3 * i + 2]);
+  set_elem(r.nu, nu ? 105.0 * nu[i] : 0.0);
+  set_elem(r.ux, -kOneOver4Pi * gu[3 * i]);
+  set_elem(r.uy, -kOneOver4Pi * gu[3 * i + 1]);
+  set_elem(r.uz, -kOneOver4Pi * gu[3 * i + 2]);
+  set_elem(r.pad0, 0.0);
+  set_elem(r.gx, kOneOver4Pi * gs[3 * i]);
+  set_elem(r.gy, kOneOver4Pi * gs[3 * i + 1]);
+  set_elem(r.gz, kOneOver4Pi * gs[3 * i + 2]);
+  set_elem(r.pad1, 0.0);
+  out[i] = r;
+}
+
+template <class E, int NV, bool PSE>
+__global__ void finalize_vjp_kernel(const double* __restrict__ part, int splits, int64_t m,
+                                    const RecG<E>* __restrict__ tgt, double* __restrict__ gx,
+                                    double* __restrict__ ga, double* __restrict__ gsig,
+                                    double* __restrict__ gnu) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double v[NV];
+  sum_splits<NV>(part, splits, m, i, v);
+  const RecG<E>& t = tgt[i];
+  const double ax = elem(t.ax), ay = elem(t.ay), az = elem(t.az);
+  const double ux = elem(t.ux), uy = elem(t.uy), uz = elem(t.uz);
+  const double sx = elem(t.gx), sy = elem(t.gy), sz = elem(t.gz);
+  const double Gx = v[VJ_GA], Gy = v[VJ_GA + 1], Gz = v[VJ_GA + 2];
+  const double Hx = v[VJ_GU], Hy = v[VJ_GU + 1], Hz = v[VJ_GU + 2];
+  // xbar += G_a x u'_k - a_k x G_u
+  gx[3 * i] = v[VJ_X] + (Gy * uz - Gz * uy) - (ay * Hz - az * Hy);
+  gx[3 * i + 1] = v[VJ_X + 1] + (Gz * ux - Gx * uz) - (az * Hx - ax * Hz);
+  gx[3 * i + 2] = v[VJ_X + 2] + (Gx * uy - Gy * ux) - (ax * Hy - ay * Hx);
+  // abar += G_a x s'_k  (+ PSE: sum k nu'_l s'_l - (sum k) nu'_k s'_k)
+  double bx = v[VJ_A] + (Gy * sz - Gz * sy);
+  double by = v[VJ_A + 1] + (Gz * sx - Gx * sz);
+  double bz = v[VJ_A + 2] + (Gx * sy - Gy * sx);
+  if constexpr (PSE) {
+    const double kn = v[VJ_K] * elem(t.nu);
+    bx += v[VJ_KS] - kn * sx;
+    by += v[VJ_KS + 1] - kn * sy;
+    bz += v[VJ_KS + 2] - kn * sz;
+  }
+  ga[3 * i] = bx;
+  ga[3 * i + 1] = by;
+  ga[3 * i + 2] = bz;
+  gsig[i] = 0.5 * v[VJ_S];
+  if (gnu) gnu[i] = PSE ? 105.0 * v[VJ_NU] : 0.0;
+}
+
+__global__ void finalize_kegrad_kernel(const double* __restrict__ part, int splits, int64_t m,
+                                       double* __restrict__ gx, double* __restrict__ ga,
+                                       double* __restrict__ gsig) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double v[7];
+  sum_splits<7>(part, splits, m, i, v);
+  const double c = 2.0 / (16.0 * kPi);
+  gx[3 * i] = c * v[0];
+  gx[3 * i + 1] = c * v[1];
+  gx[3 * i + 2] = c * v[2];
+  ga[3 * i] = c * v[3];
+  ga[3 * i + 1] = c * v[4];
+  ga[3 * i + 2] = c * v[5];
+  gsig[i] = 0.5 * c * v[6];
+}
+
 // ---- operator selection -----------------------------------------------------------------
 template <class T, bool REFINE>
 struct Ops {
@@ -336,6 +423,9 @@ struct Ops {
   using Ke = OpKe<T, REFINE>;
   using Ens = OpEns<T, REFINE>;
   using VelStretch = OpVelStretch<T, REFINE>;
+  using RhsVjp = OpRhsVjp<T, REFINE, false>;
+  using RhsVjpPse = OpRhsVjp<T, REFINE, true>;
+  using KeGrad = OpKeGrad<T, REFINE>;
 };
 
 bool is_probe(int op) { return op == VPM_OP_INDUCED_VELOCITY_AT || op == VPM_OP_VORTICITY_FIELD_AT; }
@@ -361,6 +451,12 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
       return Sweep<typename O::Ens, T>::plan(m, n, p, mpb);
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
       return Sweep<typename O::VelStretch, T>::plan(m, n, p, mpb);
+    case VPM_OP_RHS_VJP:
+      return Sweep<typename O::RhsVjp, T>::plan(m, n, p, mpb);
+    case VPM_OP_RHS_VJP_PSE:
+      return Sweep<typename O::RhsVjpPse, T>::plan(m, n, p, mpb);
+    case VPM_OP_KINETIC_ENERGY_GRAD:
+      return Sweep<typename O::KeGrad, T>::plan(m, n, p, mpb);
     default:
       return fail(VPM_ERR_ARG, "unknown op " + std::to_string(op));
   }
@@ -371,10 +467,15 @@ struct Layout {
 };
 
 template <class T>
+size_t op_record_bytes(int op) {
+  return (op == VPM_OP_RHS_VJP || op == VPM_OP_RHS_VJP_PSE) ? sizeof(RecG<T>) : sizeof(Rec<T>);
+}
+
+template <class T>
 Layout layout_for(int op, const Plan& p, int64_t m, int64_t n) {
   Layout L;
   L.src_off = 0;
-  size_t off = align_up(size_t(n > 0 ? n : 0) * sizeof(Rec<T>));
+  size_t off = align_up(size_t(n > 0 ? n : 0) * op_record_bytes<T>(op));
   L.tgt_off = off;
   if (is_probe(op)) off = align_up(off + size_t(m > 0 ? m : 0) * sizeof(Rec<T>));
   L.part_off = off;
@@ -540,6 +641,83 @@ int dispatch(const Call& c, int precision) {
       return fail(VPM_ERR_ARG, "unknown precision " + std::to_string(precision));
   }
 }
+
+struct GradCall {
+  int op;
+  const double *pos, *str, *rad, *nu, *gu, *gs;
+  int64_t n;
+  double *ox, *oa, *os, *onu;
+  void* ws;
+  size_t ws_bytes;
+  cudaStream_t st;
+};
+
+template <class T, bool REFINE>
+int run_grad(const GradCall& c) {
+  using O = Ops<T, REFINE>;
+  int rc = check_arch();
+  if (rc) return rc;
+  if (c.n == 0) return VPM_OK;
+  Plan p;
+  Layout L;
+  rc = workspace_for<T, REFINE>(c.op, c.n, c.n, &L, &p);
+  if (rc) return rc;
+  if (c.ws == nullptr) return fail(VPM_ERR_WORKSPACE, "workspace is null");
+  if (reinterpret_cast<uintptr_t>(c.ws) % kAlign != 0)
+    return fail(VPM_ERR_ALIGN, "workspace must be 256-byte aligned");
+  if (c.ws_bytes < L.total)
+    return fail(VPM_ERR_WORKSPACE, "workspace has " + std::to_string(c.ws_bytes) +
+                                       " bytes, needs " + std::to_string(L.total));
+  char* ws = static_cast<char*>(c.ws);
+  double* part = reinterpret_cast<double*>(ws + L.part_off);
+  const unsigned blocks = unsigned((c.n + 255) / 256);
+  cudaError_t e;
+  if (c.op == VPM_OP_KINETIC_ENERGY_GRAD) {
+    Rec<T>* rec = reinterpret_cast<Rec<T>*>(ws + L.src_off);
+    rc = pack<T>(c.pos, c.str, c.rad, nullptr, c.n, rec, c.st);
+    if (!rc) rc = Sweep<typename O::KeGrad, T>::launch(p, rec, c.n, 0, rec, c.n, part, c.st);
+    if (rc) return rc;
+    finalize_kegrad_kernel<<<blocks, 256, 0, c.st>>>(part, p.splits, c.n, c.ox, c.oa, c.os);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? VPM_OK : cuda_fail(e, "finalize launch");
+  }
+  RecG<T>* rec = reinterpret_cast<RecG<T>*>(ws + L.src_off);
+  pack_grad_kernel<T><<<blocks, 256, 0, c.st>>>(c.pos, c.str, c.rad, c.nu, c.gu, c.gs, c.n, rec);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "pack launch");
+  if (c.op == VPM_OP_RHS_VJP_PSE) {
+    rc = Sweep<typename O::RhsVjpPse, T>::launch(p, rec, c.n, 0, rec, c.n, part, c.st);
+    if (rc) return rc;
+    finalize_vjp_kernel<T, O::RhsVjpPse::NV, true>
+        <<<blocks, 256, 0, c.st>>>(part, p.splits, c.n, rec, c.ox, c.oa, c.os, c.onu);
+  } else {
+    rc = Sweep<typename O::RhsVjp, T>::launch(p, rec, c.n, 0, rec, c.n, part, c.st);
+    if (rc) return rc;
+    finalize_vjp_kernel<T, O::RhsVjp::NV, false>
+        <<<blocks, 256, 0, c.st>>>(part, p.splits, c.n, rec, c.ox, c.oa, c.os, c.onu);
+  }
+  e = cudaGetLastError();
+  return e == cudaSuccess ? VPM_OK : cuda_fail(e, "finalize launch");
+}
+
+int dispatch_grad(const GradCall& c, int precision) {
+  if (c.n < 0) return fail(VPM_ERR_ARG, "negative size");
+  if (c.n > 0 && (!c.pos || !c.str || !c.rad || !c.ox || !c.oa || !c.os))
+    return fail(VPM_ERR_ARG, "null pointer");
+  if (c.op != VPM_OP_KINETIC_ENERGY_GRAD && c.n > 0 && (!c.gu || !c.gs))
+    return fail(VPM_ERR_ARG, "null cotangent pointer");
+  switch (precision) {
+    case VPM_FP64:
+      return run_grad<double, false>(c);
+    case VPM_FP32C:
+      return run_grad<float2, false>(c);
+    case VPM_FP32C_REFINED:
+      return run_grad<float2, true>(c);
+    default:
+      return fail(VPM_ERR_ARG, "unknown precision " + std::to_string(precision));
+  }
+}
+
 
 // ---- scratch for the no-allocation entry point --------------------------------------------
 // Some callers may not allocate device memory at all: a solver plugin that runs inside a
@@ -796,6 +974,28 @@ int vpm_sweep_records(int op, const void* records, int64_t n, int64_t target_beg
   c.tgt_begin = target_begin;
   if (n > 0 && !records) return fail(VPM_ERR_ARG, "null records pointer");
   return dispatch(c, precision);
+}
+
+int vpm_rhs_vjp(const double* positions, const double* strengths, const double* radii,
+                const double* viscosities, int64_t n, const double* grad_velocities,
+                const double* grad_rates, double* grad_positions, double* grad_strengths,
+                double* grad_radii, double* grad_viscosities, int precision, void* workspace,
+                size_t workspace_bytes, void* stream) {
+  GradCall c{viscosities ? VPM_OP_RHS_VJP_PSE : VPM_OP_RHS_VJP, positions, strengths, radii,
+             viscosities, grad_velocities, grad_rates, n, grad_positions, grad_strengths,
+             grad_radii, grad_viscosities, workspace, workspace_bytes,
+             static_cast<cudaStream_t>(stream)};
+  return dispatch_grad(c, precision);
+}
+
+int vpm_kinetic_energy_grad(const double* positions, const double* strengths,
+                            const double* radii, int64_t n, double* grad_positions,
+                            double* grad_strengths, double* grad_radii, int precision,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+  GradCall c{VPM_OP_KINETIC_ENERGY_GRAD, positions, strengths, radii, nullptr, nullptr, nullptr,
+             n, grad_positions, grad_strengths, grad_radii, nullptr, workspace,
+             workspace_bytes, static_cast<cudaStream_t>(stream)};
+  return dispatch_grad(c, precision);
 }
 
 // Self-induced velocity without any allocation: the scratch (packed records and per-split

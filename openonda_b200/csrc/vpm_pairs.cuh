@@ -84,9 +84,20 @@ __device__ __forceinline__ Tgt<float2> make_tgt(const Rec<float2>* const* r) {
                      make_float2(a.az.x, b.az.x)};
 }
 
+// Record/lane plumbing shared by the operators on the standard 64-byte record.
+template <class V>
+struct PairOpBase {
+  static constexpr int kR = 0;  // targets per thread: 0 = the precision's default
+  using Record = Rec<V>;
+  using SrcT = Src<V>;
+  using TgtT = Tgt<V>;
+  __device__ __forceinline__ static SrcT load(const Record& r) { return load_src<V>(r); }
+  __device__ __forceinline__ static TgtT target(const Record* const* r) { return make_tgt(r); }
+};
+
 // ---- self-induced velocity: U += g (r x a_j) ------------------------------------------
 template <class V, bool REFINE>
-struct OpVel {
+struct OpVel : PairOpBase<V> {
   static constexpr int NV = 3;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
@@ -109,7 +120,7 @@ struct OpVel {
 
 // ---- probe velocity: source core sigma_j, pairs with r^2 <= 1e-8 skipped ----------------
 template <class V, bool REFINE>
-struct OpVelAt {
+struct OpVelAt : PairOpBase<V> {
   static constexpr int NV = 3;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
@@ -131,7 +142,7 @@ struct OpVelAt {
 
 // ---- probe vorticity (zeta kernel only): W += s^4 y^7 a_j, r^2 <= 1e-8 skipped ----------
 template <class V, bool REFINE>
-struct OpVortAt {
+struct OpVortAt : PairOpBase<V> {
   static constexpr int NV = 3;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
@@ -151,7 +162,7 @@ struct OpVortAt {
 
 // ---- stretching (transpose scheme): A += g (a_j - a_i),  B += f (r . (d x a_i)) r -------
 template <class V, bool REFINE>
-struct OpStretch {
+struct OpStretch : PairOpBase<V> {
   static constexpr int NV = 6;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
@@ -184,7 +195,7 @@ struct OpStretch {
 #define VPM_Y2_RCP 0
 #endif
 template <class V, bool REFINE>
-struct OpVelStretch {
+struct OpVelStretch : PairOpBase<V> {
   static constexpr int NV = 9;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
@@ -220,7 +231,7 @@ struct OpVelStretch {
 
 // ---- PSE diffusion: P += s^7 y^9 (a_j - a_i)  (nu_i applied in finalize) -----------------
 template <class V, bool REFINE>
-struct OpPse {
+struct OpPse : PairOpBase<V> {
   static constexpr int NV = 3;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
@@ -242,7 +253,7 @@ struct OpPse {
 
 // ---- enstrophy filter sum (all pairs incl. i == j): V += (x + 2.2 s^2) y^3 a_j ---------
 template <class V, bool REFINE>
-struct OpEns {
+struct OpEns : PairOpBase<V> {
   static constexpr int NV = 3;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
@@ -261,7 +272,7 @@ struct OpEns {
 
 // ---- kinetic energy (j != i): K += (y + s^2 y^3) a_j + y^3 (r . a_j) r ------------------
 template <class V, bool REFINE>
-struct OpKe {
+struct OpKe : PairOpBase<V> {
   static constexpr int NV = 3;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t* i, int64_t j) {

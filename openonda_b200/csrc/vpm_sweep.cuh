@@ -26,12 +26,12 @@ namespace vpm {
 #endif
 constexpr int kCarryWindow = VPM_CARRY_WINDOW;
 
-template <class V>
+template <class R>
 struct SweepArgs {
-  const Rec<V>* tgt;
+  const R* tgt;
   int64_t m;
   int64_t tgt_offset;  // global index of tgt[0] among the sources (self-pair exclusion)
-  const Rec<V>* src;
+  const R* src;
   int64_t n;
   int64_t chunk;  // sources per split (multiple of kCarryWindow unless it is the last)
   double* partial;
@@ -49,25 +49,26 @@ constexpr int kSrcUnroll = VPM_SRC_UNROLL;
 
 // Dynamic shared memory of one block: the source-tile ring, then (FP32 with shared-memory
 // carries) the FP64 carries laid out [value][target][thread] for conflict-free access.
-template <class V, int NV, int R, int THREADS, int TILE, int STAGES>
+template <class V, class Rec_, int NV, int R, int THREADS, int TILE, int STAGES>
 constexpr size_t sweep_smem_bytes() {
-  return size_t(STAGES) * TILE * sizeof(Rec<V>) +
+  return size_t(STAGES) * TILE * sizeof(Rec_) +
          ((LaneTraits<V>::kLanes == 2 && VPM_SMEM_CARRY) ? size_t(NV) * R * THREADS * 8 : 0);
 }
 
 template <class Op, class V, int R, int THREADS, int TILE, int STAGES>
 __global__ void __launch_bounds__(THREADS)
-sweep_kernel(const SweepArgs<V> a) {
+sweep_kernel(const SweepArgs<typename Op::Record> a) {
+  using RecT = typename Op::Record;
   constexpr int NV = Op::NV;
   constexpr int L = LaneTraits<V>::kLanes;
   constexpr int P = R / L;
   constexpr bool kCarry = (L == 2);
   constexpr bool kSmemCarry = kCarry && VPM_SMEM_CARRY;
-  constexpr uint32_t kRecBytes = sizeof(Rec<V>);
+  constexpr uint32_t kRecBytes = sizeof(RecT);
   static_assert(R % L == 0, "targets per thread must fill whole lanes");
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  Rec<V>* tiles = reinterpret_cast<Rec<V>*>(smem_raw);
+  RecT* tiles = reinterpret_cast<RecT*>(smem_raw);
   __shared__ __align__(8) uint64_t full_bar[STAGES];
 
   const int tid = threadIdx.x;
@@ -77,12 +78,12 @@ sweep_kernel(const SweepArgs<V> a) {
   const int64_t count = (j1 > j0) ? (j1 - j0) : 0;
   const int ntiles = static_cast<int>((count + TILE - 1) / TILE);
 
-  Tgt<V> tg[P];
+  typename Op::TgtT tg[P];
   int64_t ti[R];  // local target index
   int64_t gi[R];  // global index among the sources
   V acc[P][NV];
   double car[(kCarry && !kSmemCarry) ? R : 1][NV];
-  double* scar = reinterpret_cast<double*>(smem_raw + size_t(STAGES) * TILE * sizeof(Rec<V>));
+  double* scar = reinterpret_cast<double*>(smem_raw + size_t(STAGES) * TILE * sizeof(RecT));
   if constexpr (kSmemCarry) {
 #pragma unroll
     for (int v = 0; v < NV; ++v)
@@ -91,7 +92,7 @@ sweep_kernel(const SweepArgs<V> a) {
   }
 #pragma unroll
   for (int p = 0; p < P; ++p) {
-    const Rec<V>* recs[L];
+    const RecT* recs[L];
 #pragma unroll
     for (int k = 0; k < L; ++k) {
       const int r = p * L + k;
@@ -99,7 +100,7 @@ sweep_kernel(const SweepArgs<V> a) {
       gi[r] = ti[r] + a.tgt_offset;
       recs[k] = a.tgt + (ti[r] < a.m ? ti[r] : a.m - 1);
     }
-    tg[p] = make_tgt(recs);
+    tg[p] = Op::target(recs);
 #pragma unroll
     for (int v = 0; v < NV; ++v) lane_zero(acc[p][v]);
   }
@@ -132,7 +133,7 @@ sweep_kernel(const SweepArgs<V> a) {
   for (int t = 0; t < ntiles; ++t) {
     const int s = t % STAGES;
     const bool ok = mbar_wait_bounded(&full_bar[s], static_cast<uint32_t>((t / STAGES) & 1));
-    const Rec<V>* tile = tiles + s * TILE;
+    const RecT* tile = tiles + s * TILE;
     const int64_t jt = j0 + static_cast<int64_t>(t) * TILE;
     const int64_t left = count - static_cast<int64_t>(t) * TILE;
     const int cnt = static_cast<int>(left < TILE ? left : TILE);
@@ -141,7 +142,7 @@ sweep_kernel(const SweepArgs<V> a) {
         const int e = (w + kCarryWindow < cnt) ? w + kCarryWindow : cnt;
 #pragma unroll kSrcUnroll
         for (int j = w; j < e; ++j) {
-          const Src<V> src = load_src<V>(tile[j]);
+          const typename Op::SrcT src = Op::load(tile[j]);
 #pragma unroll
           for (int p = 0; p < P; ++p) Op::pair(tg[p], acc[p], src, &gi[p * L], jt + j);
         }
