@@ -1,0 +1,291 @@
+"""The five benchmark workloads, run through the public API; one JSON line per result.
+
+    python -m openonda_b200.workloads {config1,config2,config3,config4,config5,stepkernels} [opts]
+
+config1  ring N=8192 (64 x 128 torus lattice), FP64, one DNS+PSE RK4 step at dt=0.01,
+         compared with the CPU oracle's restatement of the reference step.
+config2  leapfrogging rings N=131072, FP32-compensated DNS+PSE, RK4 dt=0.005, nu=1e-4;
+         velocity/stretching error vs FP64 at steps 1, 50, 200; FP64 circulation and
+         linear-impulse drift.
+config3  random-cloud throughput sweep N = 2^14 .. 2^21: fused velocity + stretching,
+         FP32c vs FP64 Gpairs/s and error.
+config4  differentiation: perturbed ring N=65536, FP32c, loss = FP64-summed kinetic energy
+         after 50 RK4 steps at dt=0.01, checkpoint every 10 steps; gradients w.r.t. initial
+         positions, strengths and cores vs the FP64 adjoint and vs FP64 central differences
+         (h=1e-6) on 64 random coordinates.
+config5  dynamic-LES ring N=2^20, FP32c, PSE, RK4 dt=0.002: time per step, Gpairs/s, error vs
+         FP64 at the last step.
+stepkernels  GB/s of the element-wise step kernels (RK stage, RK4 combine, BDF) at N=2^22.
+
+All inputs are the seeded synthetic fields of :mod:`openonda_b200.configs`.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import configs, kernels
+
+
+def _emit(d):
+    print(json.dumps(d), flush=True)
+
+
+def _rel(a, b):
+    a = a if isinstance(a, torch.Tensor) else torch.as_tensor(a)
+    b = b if isinstance(b, torch.Tensor) else torch.as_tensor(b)
+    return float((a - b).abs().max() / b.abs().max())
+
+
+class _Timer:
+    def __init__(self):
+        self.e0 = torch.cuda.Event(enable_timing=True)
+        self.e1 = torch.cuda.Event(enable_timing=True)
+
+    def __enter__(self):
+        torch.cuda.synchronize()
+        self.e0.record()
+        return self
+
+    def __exit__(self, *exc):
+        self.e1.record()
+        self.e1.synchronize()
+        self.ms = self.e0.elapsed_time(self.e1)
+
+
+def _system(field, precision, **kw):
+    from .vpm.vpmModule import ParticleSystem
+
+    ps = ParticleSystem(monitor_variables=[], backup_frequency=10 ** 9, precision=precision,
+                        **kw)
+    ps.add_particle_field(field.positions, np.zeros_like(field.positions), field.strengths,
+                          field.radii, field.viscosities)
+    return ps
+
+
+def _step(ps):
+    ps.update_velocities()
+    ps.update_strengths()
+    ps.update_state()
+
+
+def config1(args):
+    import oracle
+    from oracle.vpm_step import StepOracle
+
+    f = configs.ring_8192()
+    kw = dict(flow_model="DNS", viscous_scheme="PSE", time_integration_method="RK4",
+              time_step_size=0.01)
+    warm = _system(f, "fp64", **kw)
+    _step(warm)
+    ps = _system(f, "fp64", **kw)
+    with _Timer() as t:
+        _step(ps)
+    t0 = time.perf_counter()
+    so = StepOracle(oracle.gpu, f.positions, f.strengths, f.radii, f.viscosities, **kw)
+    so.step()
+    t_cpu = time.perf_counter() - t0
+    n = f.n
+    _emit({"config": "config1", "workload": f.description, "n": n,
+           "b200_ms_per_step": round(t.ms, 3), "sweeps_per_step": 5,
+           "oracle_cpu_s_per_step": round(t_cpu, 2), "oracle_threads": oracle.num_threads(),
+           "rel_err_positions": _rel(torch.from_numpy(ps.get_particle_positions()),
+                                     torch.from_numpy(so.x)),
+           "rel_err_strengths": _rel(torch.from_numpy(ps.get_particle_strengths()),
+                                     torch.from_numpy(so.a)),
+           "rel_err_velocities": _rel(torch.from_numpy(ps.get_particle_velocities()),
+                                      torch.from_numpy(so.u))})
+
+
+def _errors_vs_fp64(ps):
+    x, a, s = ps.positions, ps.strengths, ps.radii
+    x32 = x.float().double()
+    a32 = a.float().double()
+    s32 = s.float().double()
+    u64, g64 = kernels.velocity_and_strength_gradients(x32, a32, s32, precision="fp64")
+    u32, g32 = kernels.velocity_and_strength_gradients(x32, a32, s32, precision="fp32c")
+    return _rel(u32, u64), _rel(g32, g64)
+
+
+def config2(args):
+    f = configs.leapfrog_rings()
+    ps = _system(f, "fp32c", flow_model="DNS", viscous_scheme="PSE",
+                 time_integration_method="RK4", time_step_size=0.005)
+    d0 = ps._diagnostics()
+    steps = args.steps or 200
+    report = {1, 50, steps}
+    rows = []
+    t_total = 0.0
+    for k in range(1, steps + 1):
+        with _Timer() as t:
+            _step(ps)
+        t_total += t.ms
+        if k in report:
+            eu, eg = _errors_vs_fp64(ps)
+            d = ps._diagnostics()
+            imp0 = np.linalg.norm(d0[4:7])
+            rows.append({"step": k, "rel_err_velocity": eu, "rel_err_stretching": eg,
+                         "circulation_drift": float((d[0] - d0[0]) / d0[0]),
+                         "linear_impulse_drift": float(np.linalg.norm(d[4:7] - d0[4:7]) / imp0)})
+    n = f.n
+    pairs = 5.0 * n * n  # fused + PSE + 3 RK stages
+    _emit({"config": "config2", "workload": f.description, "n": n, "steps": steps,
+           "precision": "fp32c", "ms_per_step": round(t_total / steps, 3),
+           "gpairs_per_s": round(pairs / (t_total / steps / 1e3) / 1e9, 1), "checkpoints": rows})
+
+
+def config3(args):
+    sizes = args.sizes or [1 << k for k in range(14, 22)]
+    for n in sizes:
+        f = configs.random_cloud(n, seed=0)
+        r = lambda z: torch.from_numpy(np.asarray(z, np.float32).astype(np.float64)).cuda()
+        x, a, s = r(f.positions), r(f.strengths), r(f.radii)
+        out = {}
+        res = {}
+        for prec in ("fp32c", "fp64"):
+            kernels.velocity_and_strength_gradients(x, a, s, precision=prec)
+            reps = 5 if (prec == "fp32c" or n <= (1 << 18)) else 1
+            with _Timer() as t:
+                for _ in range(reps):
+                    out[prec] = kernels.velocity_and_strength_gradients(x, a, s,
+                                                                        precision=prec)
+            res[prec] = n * n / (t.ms / reps / 1e3) / 1e9
+        _emit({"config": "config3", "n": n, "fp32c_gpairs_s": round(res["fp32c"], 1),
+               "fp64_gpairs_s": round(res["fp64"], 1),
+               "speedup": round(res["fp32c"] / res["fp64"], 2),
+               "rel_err_velocity": _rel(out["fp32c"][0], out["fp64"][0]),
+               "rel_err_stretching": _rel(out["fp32c"][1], out["fp64"][1])})
+
+
+def config4(args):
+    from . import autodiff
+
+    f = configs.perturbed_ring()
+    r = lambda z: torch.from_numpy(np.asarray(z, np.float32).astype(np.float64)).cuda()
+    x0, a0, s0 = r(f.positions), r(f.strengths), r(f.radii)
+    steps, dt, every = args.steps or 50, 0.01, 10
+
+    def grad(prec):
+        x, a, s = (z.clone().requires_grad_() for z in (x0, a0, s0))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        xT, aT = autodiff.trajectory(x, a, s, None, dt, steps, prec, checkpoint_every=every)
+        e = autodiff.kinetic_energy(xT, aT, s, prec)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        g = torch.autograd.grad(e, (x, a, s))
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        return float(e), g, t1 - t0, t2 - t1
+
+    e32, g32, f32, b32 = grad("fp32c")
+    e64, g64, f64, b64 = grad("fp64")
+
+    def loss64(x, a, s):
+        with torch.no_grad():
+            xT, aT = autodiff.trajectory(x, a, s, None, dt, steps, "fp64")
+            return float(kernels.total_kinetic_energy(xT, aT, s, precision="fp64"))
+
+    rng = np.random.default_rng(2024)
+    n_fd = args.fd or 64
+    h = 1e-6
+    fd_err32, fd_err64 = [], []
+    bases = (x0, a0, s0)
+    for q in range(n_fd):
+        which = q % 3
+        base = bases[which]
+        idx = tuple(int(rng.integers(0, d)) for d in base.shape)
+        step = h * (float(a0.abs().max()) if which == 1 else 1.0)
+        bp, bm = base.clone(), base.clone()
+        bp[idx] += step
+        bm[idx] -= step
+        args_p, args_m = list(bases), list(bases)
+        args_p[which], args_m[which] = bp, bm
+        fd = (loss64(*args_p) - loss64(*args_m)) / (2 * step)
+        scale = float(g64[which].abs().max())
+        fd_err64.append(abs(float(g64[which][idx]) - fd) / scale)
+        fd_err32.append(abs(float(g32[which][idx]) - fd) / scale)
+    _emit({"config": "config4", "workload": f.description, "n": f.n, "steps": steps,
+           "dt": dt, "checkpoint_every": every, "loss_fp32c": e32, "loss_fp64": e64,
+           "grad_rel_err_fp32c_vs_fp64": {k: _rel(g32[i], g64[i])
+                                           for i, k in enumerate(("x", "alpha", "sigma"))},
+           "fd_coordinates": n_fd, "fd_h": h,
+           "fd_max_err_fp64_adjoint": max(fd_err64), "fd_max_err_fp32c_adjoint": max(fd_err32),
+           "fp32c_forward_s": round(f32, 2), "fp32c_backward_s": round(b32, 2),
+           "fp64_forward_s": round(f64, 2), "fp64_backward_s": round(b64, 2)})
+
+
+def config5(args):
+    f = configs.les_ring()
+    steps = args.steps or 100
+    ps = _system(f, "fp32c", flow_model="LES", viscous_scheme="PSE",
+                 time_integration_method="RK4", time_step_size=0.002)
+    t_total = 0.0
+    for k in range(steps):
+        with _Timer() as t:
+            _step(ps)
+        t_total += t.ms
+    eu, eg = _errors_vs_fp64(ps)
+    n = f.n
+    sweeps = 7.0  # fused vel+stretch, vorticity, enstrophy, PSE, 3 RK stages
+    _emit({"config": "config5", "workload": f.description, "n": n, "steps": steps,
+           "precision": "fp32c", "ms_per_step": round(t_total / steps, 1),
+           "gpairs_per_s": round(sweeps * n * n / (t_total / steps / 1e3) / 1e9, 1),
+           "rel_err_velocity_last_step": eu, "rel_err_stretching_last_step": eg,
+           "cnu": ps.Cnu})
+
+
+def stepkernels(args):
+    from . import _lib
+
+    lib = _lib.load()
+    n = args.n or (1 << 22)
+    dev = torch.device("cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    x, k1, k2, k3, k4 = (torch.rand((n, 3), dtype=torch.float64, device=dev) for _ in range(5))
+    out = torch.empty_like(x)
+    h1, h2, h3 = (torch.rand_like(x) for _ in range(3))
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    cases = {
+        "axpy (RK stage)": (lambda: lib.vpm_axpy(x.data_ptr(), k1.data_ptr(), 0.005, x.numel(),
+                                                 out.data_ptr(), st), 72),
+        "rk4_combine": (lambda: lib.vpm_rk4_combine(x.data_ptr(), k1.data_ptr(), k2.data_ptr(),
+                                                    k3.data_ptr(), k4.data_ptr(), 0.01,
+                                                    x.numel(), out.data_ptr(), st), 144),
+        "bdf (BDF4 step)": (lambda: lib.vpm_bdf_update(out.data_ptr(), h1.data_ptr(),
+                                                       h2.data_ptr(), h3.data_ptr(),
+                                                       k1.data_ptr(), x.numel(), 5, 0.01, st),
+                            216),
+    }
+    for name, (fn, bytes_per) in cases.items():
+        fn()
+        times = []
+        for _ in range(10):
+            flush.fill_(0)
+            with _Timer() as t:
+                fn()
+            times.append(t.ms)
+        ms = float(np.median(times))
+        _emit({"kernel": name, "n": n, "bytes": bytes_per * n, "ms": round(ms, 4),
+               "gb_s": round(bytes_per * n / (ms / 1e3) / 1e9, 1)})
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("workload", choices=["config1", "config2", "config3", "config4", "config5",
+                                         "stepkernels"])
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--fd", type=int, default=None)
+    ap.add_argument("--n", type=int, default=None)
+    ap.add_argument("--sizes", type=int, nargs="*", default=None)
+    args = ap.parse_args()
+    globals()[args.workload](args)
+
+
+if __name__ == "__main__":
+    main()
