@@ -353,6 +353,33 @@ def main():
         fp64_dropin = float(n) * n / tdi / 1e9
         del xa, aa, sa
 
+    # ---- the reference's GPU algorithm (one thread per target, FP64 pow), same box ----
+    naive = None
+    if world == 1:
+        from openonda_b200 import _lib
+
+        nn = min(n, 131072)
+        xa = torch.from_numpy(x_h[:nn]).to(dev)
+        aa = torch.from_numpy(a_h[:nn]).to(dev)
+        sa = torch.from_numpy(s_h[:nn]).to(dev)
+        outn = torch.empty((nn, 3), dtype=torch.float64, device=dev)
+        lib = _lib.load()
+        stream = torch.cuda.current_stream(dev).cuda_stream
+
+        def naive_step():
+            for which in (0, 1):
+                _lib.check(lib.vpm_naive_reference_kernel(which, xa.data_ptr(), aa.data_ptr(),
+                                                          sa.data_ptr(), nn, outn.data_ptr(),
+                                                          stream))
+            return outn
+
+        tn, _, _ = timed(naive_step, 1, 1)
+        naive = {"n": nn, "gpairs_s": round(float(nn) * nn / tn / 1e9, 3),
+                 "kernels": "velocity + stretching, one thread per target, 512 threads/block, "
+                            "FP64 pow, global-memory sources (the reference's Numba-CUDA "
+                            "structure restated in CUDA C++)"}
+        del xa, aa, sa, outn
+
     # ---- end to end through the public API, host buffers (pinned), copies timed ----
     xp = torch.from_numpy(x_h[start:stop]).pin_memory()
     ap_ = torch.from_numpy(a_h[start:stop]).pin_memory()
@@ -415,6 +442,9 @@ def main():
                      "speedup_vs_fp64_dropin":
                          None if fp64_dropin is None else round(value / fp64_dropin, 3)},
             "rel_err_vs_fp64": {"velocity": err_u, "stretching": err_g},
+            "reference_algorithm_gpu": naive,
+            "speedup_vs_reference_algorithm_gpu":
+                None if naive is None else round(value / naive["gpairs_s"], 1),
             "roofline": {"bound": "fp32", "achieved": round(achieved, 3),
                          "peak": round(peak, 3), "unit": "TFLOP/s",
                          "frac": round(achieved / peak, 4), "traffic": tr,

@@ -215,6 +215,11 @@ int vpm_selfinduced_velocity_noalloc(const double* positions, const double* stre
                                      int precision, void* stream);
 
 /* ---- measurement helpers -------------------------------------------------------------- */
+/* The reference's GPU algorithm restated for comparison (ParticlesPhysicsCuda.py:133-191 when
+ * which = 0, :375-445 when which = 1): one thread per target, 512 threads per block, sources
+ * read from global memory, FP64 powers.  bench.py times it as the reference-algorithm GPU bar. */
+int vpm_naive_reference_kernel(int which, const double* positions, const double* strengths,
+                               const double* radii, int64_t n, double* out, void* stream);
 /* FP32 FMA (fp64 != 0: FP64 FMA) throughput kernel: blocks x threads threads each run
  * `iters` iterations of 16 independent FMA chains; one value per thread lands in `sink`
  * (blocks*threads floats or doubles).  FMA count = blocks*threads*iters*16. */

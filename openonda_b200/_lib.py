@@ -73,6 +73,7 @@ SIGNATURES = {
     "vpm_les_update": ([_P, _P, _P, _I64, _I, _P, _P, _P, _P, _SZ, _P], _I),
     "vpm_relax_strengths": ([_P, _P, _I64, ctypes.c_double, _P], _I),
     "vpm_particle_diagnostics": ([_P, _P, _I64, _P, _P], _I),
+    "vpm_naive_reference_kernel": ([_I, _P, _P, _P, _I64, _P, _P], _I),
     "vpm_launch_fma_peak": ([_I, _I, _I, _I, _P, _P], _I),
 }
 

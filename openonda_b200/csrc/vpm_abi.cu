@@ -1044,3 +1044,6 @@ int vpm_launch_fma_peak(int fp64, int blocks, int threads, int iters, void* sink
 
 // Element-wise time-step kernels and O(N) diagnostics (same translation unit).
 #include "vpm_step.cuh"
+
+// The reference's GPU algorithm restated (measurement only).
+#include "vpm_naive.cuh"

@@ -264,3 +264,22 @@ def test_records_target_shards_reassemble():
         assert normwise(torch.cat(parts_u).cpu().numpy(), u_full.cpu().numpy()) <= 1e-14
         assert normwise(torch.cat(parts_g).cpu().numpy(), g_full.cpu().numpy()) <= 1e-14
         assert abs(ke - float(ke_full)) <= 1e-12 * abs(float(ke_full))
+
+
+def test_naive_reference_kernels_match_oracle():
+    """The measurement-only restatement of the reference's GPU kernels computes the same sums."""
+    import torch
+
+    from openonda_b200 import _lib, configs
+
+    f = configs.random_cloud(1500, seed=31)
+    f.radii *= 5
+    lib = _lib.load()
+    x, a, s = (torch.from_numpy(z).cuda() for z in (f.positions, f.strengths, f.radii))
+    out = torch.empty((1500, 3), dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    for which, ref in ((0, oracle.gpu.get_selfinduced_velocity),
+                       (1, oracle.gpu.get_strength_gradients)):
+        _lib.check(lib.vpm_naive_reference_kernel(which, x.data_ptr(), a.data_ptr(),
+                                                  s.data_ptr(), 1500, out.data_ptr(), st))
+        assert normwise(out.cpu().numpy(), ref(f.positions, f.strengths, f.radii)) <= 1e-13
