@@ -66,6 +66,10 @@ const char* vpm_last_error(void);
 int vpm_check_device(void);
 /* Read (and optionally clear) the device error word: bit 0 = a bounded wait timed out. */
 int vpm_device_errors(int* out, int clear);
+/* Failure-detection self-test: one block waits on an mbarrier phase that never completes; the
+ * bounded wait gives up after ~1 s, sets bit 0 of the device error word, writes 1 to the
+ * device int `timed_out` and the kernel returns (no fault, the context stays usable). */
+int vpm_selftest_bounded_wait(int* timed_out, void* stream);
 /* Scratch bytes `op` needs for m targets and n sources (m = n for self sums). */
 size_t vpm_workspace_bytes(int op, int precision, int64_t m, int64_t n);
 /* Launch plan of `op`: target blocks, source splits, threads/block, targets/thread. */

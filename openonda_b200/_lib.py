@@ -47,6 +47,7 @@ SIGNATURES = {
     "vpm_last_error": ([], ctypes.c_char_p),
     "vpm_check_device": ([], _I),
     "vpm_device_errors": ([ctypes.POINTER(_I), _I], _I),
+    "vpm_selftest_bounded_wait": ([_P, _P], _I),
     "vpm_workspace_bytes": ([_I, _I, _I64, _I64], _SZ),
     "vpm_plan_info": ([_I, _I, _I64, _I64, ctypes.POINTER(_I64), ctypes.POINTER(_I),
                        ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),

@@ -737,6 +737,24 @@ std::unordered_map<int, void*> g_noalloc_addr;  // device -> device address of t
 
 int noalloc_scratch(void** out);
 
+// ---- bounded-wait self-test -----------------------------------------------------------------
+// One block waits on an mbarrier phase that nothing completes (16 transaction bytes are
+// expected and never sent).  mbar_wait_bounded gives up after its time limit, records
+// VPM_DEVERR_WAIT_TIMEOUT and the kernel returns: the same path a sweep takes when a tile copy
+// never lands.  No copy is issued, so nothing is in flight when the block exits.
+__global__ void bounded_wait_selftest_kernel(int* __restrict__ result) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 16);
+  __syncthreads();
+  const bool ok = mbar_wait_bounded(&bar, 0);
+  if (__syncthreads_or(!ok) && threadIdx.x == 0) result[0] = 1;
+}
+
 // ---- FMA throughput kernels ------------------------------------------------------------
 template <class T>
 __global__ void fma_peak_kernel(int iters, T* sink) {
@@ -1024,6 +1042,15 @@ int vpm_selfinduced_velocity_noalloc(const double* positions, const double* stre
          static_cast<cudaStream_t>(stream)};
   c.max_partial_bytes = kNoAllocScratchBytes - kNoAllocRecordBytes;
   return dispatch(c, precision);
+}
+
+int vpm_selftest_bounded_wait(int* timed_out, void* stream) {
+  if (!timed_out) return fail(VPM_ERR_ARG, "null result pointer");
+  int rc = check_arch();
+  if (rc) return rc;
+  bounded_wait_selftest_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(timed_out);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? VPM_OK : cuda_fail(e, "selftest launch");
 }
 
 int vpm_launch_fma_peak(int fp64, int blocks, int threads, int iters, void* sink, void* stream) {
