@@ -204,6 +204,48 @@ int vpm_relax_strengths(double* strengths, const double* vorticity, int64_t n, d
 int vpm_particle_diagnostics(const double* positions, const double* strengths, int64_t n,
                              double* out10, void* stream);
 
+/* ---- initial conditions and lattices on the device ------------------------------------
+ * Restate OpenONDA/utilities/vpm_flow_models.py and vpm_solver_helper.py; the reference builds
+ * these fields with host numpy/numba.  All arrays are device, FP64, AoS (n,3) or (n,). */
+
+/* Workspace (256-byte aligned) needed by vpm_ic_vortex_ring for n particles. */
+size_t vpm_ic_workspace_bytes(int64_t n);
+/* vortex_ring_vpm (vpm_flow_models.py:87-163): Gaussian-core ring of radius ring_radius in the
+ * y-z plane around center, Widnall-type core displacement epsilon_w cos/sin(phase_w + n_w
+ * theta); strengths = omega * volume, rescaled so that sum|alpha| = 2 pi R Gamma; radii and
+ * viscosities filled with the particle values.  Velocities (zero in the reference) are the
+ * caller's.  A field whose total |alpha| is zero gives non-finite strengths (the reference
+ * raises ZeroDivisionError). */
+int vpm_ic_vortex_ring(const double* positions, const double* volumes, int64_t n,
+                       double particle_radius, double particle_viscosity, double center_x,
+                       double center_y, double center_z, double ring_radius,
+                       double ring_strength, double ring_thickness, double epsilon_w,
+                       double phase_w, double n_w, double* strengths, double* radii,
+                       double* viscosities, void* workspace, size_t workspace_bytes,
+                       void* stream);
+/* lamb_oseen_vpm (vpm_flow_models.py:14-83): axial (z) vorticity of a Gaussian core around
+ * (center_x + eps sin(phase + N z), center_y + eps cos(phase + N z)). */
+int vpm_ic_lamb_oseen(const double* positions, const double* volumes, int64_t n,
+                      double particle_radius, double particle_viscosity, double center_x,
+                      double center_y, double center_z, double vortex_strength,
+                      double core_radius, double epsilon_w, double phase_w, double n_w,
+                      double* strengths, double* radii, double* viscosities, void* stream);
+/* Lattices.  box_limits / center are HOST arrays ([xmin,xmax,ymin,ymax,zmin,zmax] / 3).  The
+ * point count is written to *count; with points == volumes == NULL nothing is launched (size
+ * query), otherwise capacity (points) must be >= *count.
+ * get_rectangular_point_distribuition (dims 3) / get_2D_rectangular_point_distribuition
+ * (dims 2, z = 0), vpm_solver_helper.py:21-117: */
+int vpm_lattice_rectangular(const double* box_limits, double spacing, int dims,
+                            double* points, double* volumes, int64_t capacity, int64_t* count,
+                            void* stream);
+/* get_hexagonal_point_distribution, vpm_solver_helper.py:120-161: */
+int vpm_lattice_hexagonal(const double* box_limits, double spacing, double* points,
+                          double* volumes, int64_t capacity, int64_t* count, void* stream);
+/* get_cylindrical_point_distribuition, vpm_solver_helper.py:164-253; axis 0/1/2 = 'x'/'y'/'z': */
+int vpm_lattice_cylindrical(double particle_distance, double radius, double height,
+                            const double* center, int axis, double* points, double* volumes,
+                            int64_t capacity, int64_t* count, void* stream);
+
 /* ---- no-allocation variant ------------------------------------------------------------ */
 #define VPM_NOALLOC_MAX_N 32768
 #define VPM_NOALLOC_SCRATCH_BYTES (8u << 20)

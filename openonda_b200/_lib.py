@@ -40,6 +40,7 @@ _P = ctypes.c_void_p
 _I64 = ctypes.c_int64
 _I = ctypes.c_int
 _SZ = ctypes.c_size_t
+_D = ctypes.c_double
 
 # name -> (argtypes, restype)
 SIGNATURES = {
@@ -74,6 +75,13 @@ SIGNATURES = {
     "vpm_les_update": ([_P, _P, _P, _I64, _I, _P, _P, _P, _P, _SZ, _P], _I),
     "vpm_relax_strengths": ([_P, _P, _I64, ctypes.c_double, _P], _I),
     "vpm_particle_diagnostics": ([_P, _P, _I64, _P, _P], _I),
+    "vpm_ic_workspace_bytes": ([_I64], _SZ),
+    "vpm_ic_vortex_ring": ([_P, _P, _I64] + [_D] * 11 + [_P, _P, _P, _P, _SZ, _P], _I),
+    "vpm_ic_lamb_oseen": ([_P, _P, _I64] + [_D] * 10 + [_P, _P, _P, _P], _I),
+    "vpm_lattice_rectangular": ([_P, _D, _I, _P, _P, _I64, ctypes.POINTER(_I64), _P], _I),
+    "vpm_lattice_hexagonal": ([_P, _D, _P, _P, _I64, ctypes.POINTER(_I64), _P], _I),
+    "vpm_lattice_cylindrical": ([_D, _D, _D, _P, _I, _P, _P, _I64, ctypes.POINTER(_I64), _P],
+                                _I),
     "vpm_naive_reference_kernel": ([_I, _P, _P, _P, _I64, _P, _P], _I),
     "vpm_launch_fma_peak": ([_I, _I, _I, _I, _P, _P], _I),
 }

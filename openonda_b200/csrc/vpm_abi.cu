@@ -44,13 +44,18 @@ struct Cfg;
 #ifndef VPM_FP32_THREADS
 #define VPM_FP32_THREADS 128
 #endif
+#ifndef VPM_FP32_MINB
+#define VPM_FP32_MINB 1
+#endif
+// MINB: resident blocks per SM requested from the register allocator (launch bounds).
 template <>
 struct Cfg<float2> {
-  static constexpr int R = VPM_FP32_R, THREADS = VPM_FP32_THREADS, TILE = 256, STAGES = 2;
+  static constexpr int R = VPM_FP32_R, THREADS = VPM_FP32_THREADS, TILE = 256, STAGES = 2,
+                       MINB = VPM_FP32_MINB;
 };
 template <>
 struct Cfg<double> {
-  static constexpr int R = 2, THREADS = 128, TILE = 128, STAGES = 2;
+  static constexpr int R = 2, THREADS = 128, TILE = 128, STAGES = 2, MINB = 1;
 };
 
 constexpr int kMaxSplits = 64;
@@ -115,7 +120,7 @@ struct Sweep {
   static constexpr size_t kSmem =
       sweep_smem_bytes<T, RecT, Op::NV, R, C::THREADS, TILE, C::STAGES>();
   static void* kernel() {
-    return reinterpret_cast<void*>(&sweep_kernel<Op, T, R, C::THREADS, TILE, C::STAGES>);
+    return reinterpret_cast<void*>(&sweep_kernel<Op, T, R, C::THREADS, TILE, C::STAGES, C::MINB>);
   }
 
   static int plan(int64_t m, int64_t n, Plan* p, size_t max_partial_bytes = kMaxPartialBytes) {
@@ -182,7 +187,7 @@ struct Sweep {
                     const RecT* src, int64_t n, double* partial, cudaStream_t st) {
     SweepArgs<RecT> a{tgt, m, tgt_offset, src, n, p.chunk, partial};
     dim3 grid(unsigned(p.tblocks), unsigned(p.splits));
-    sweep_kernel<Op, T, R, C::THREADS, TILE, C::STAGES><<<grid, C::THREADS, p.smem, st>>>(a);
+    sweep_kernel<Op, T, R, C::THREADS, TILE, C::STAGES, C::MINB><<<grid, C::THREADS, p.smem, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
     return VPM_OK;
@@ -1074,3 +1079,6 @@ int vpm_launch_fma_peak(int fp64, int blocks, int threads, int iters, void* sink
 
 // The reference's GPU algorithm restated (measurement only).
 #include "vpm_naive.cuh"
+
+// Initial conditions and particle lattices on the device.
+#include "vpm_ic.cuh"

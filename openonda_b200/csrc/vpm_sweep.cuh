@@ -55,8 +55,8 @@ constexpr size_t sweep_smem_bytes() {
          ((LaneTraits<V>::kLanes == 2 && VPM_SMEM_CARRY) ? size_t(NV) * R * THREADS * 8 : 0);
 }
 
-template <class Op, class V, int R, int THREADS, int TILE, int STAGES>
-__global__ void __launch_bounds__(THREADS)
+template <class Op, class V, int R, int THREADS, int TILE, int STAGES, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
 sweep_kernel(const SweepArgs<typename Op::Record> a) {
   using RecT = typename Op::Record;
   constexpr int NV = Op::NV;

@@ -78,3 +78,14 @@ def scalar_close(got, ref, rel, scale, abs_frac=1e-15):
         return bool(np.isnan(got))
     d = abs(got - ref)
     return d <= rel * abs(ref) or d <= abs_frac * scale
+
+
+def ic_cases():
+    """The seeded initial-condition / lattice cases that tests/golden/ic.npz was made from."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location(
+        "make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.ic_cases()

@@ -19,6 +19,9 @@ It executes the reference's own code and writes ``tests/golden/*.npz``:
 * ``steps_cpu.npz``    -- ``vpmModule.ParticleSystem`` (processing_unit='CPU') trajectories.
 * ``steps_gpu.npz``    -- ``vpmModule.ParticleSystem`` with the Numba-CUDA module under the
   simulator (GPU semantics), small N.
+* ``ic.npz``           -- ``OpenONDA/utilities/vpm_flow_models.py`` (vortex_ring_vpm,
+  lamb_oseen_vpm) and ``vpm_solver_helper.py`` (rectangular, 2-D rectangular, hexagonal and
+  cylindrical lattices) on the seeded cases of ``ic_cases()``.
 * ``step_ring8192.npz`` -- one DNS+PSE+RK4 step of the 8192-particle ring through the
   reference ``ParticleSystem`` sequencing with the GPU-semantics oracle kernels injected as
   its physics module (the simulator is too slow at this size).
@@ -346,6 +349,61 @@ def make_step_ring8192(ref):
     np.savez_compressed(os.path.join(HERE, "step_ring8192.npz"), **out)
 
 
+def ic_cases():
+    """Seeded inputs for the initial-condition and lattice generators (shared with tests)."""
+    rng = np.random.default_rng(77)
+    ring_pts = rng.uniform(-1.3, 1.3, size=(3000, 3))
+    ring_pts[:, 0] *= 0.3
+    return {
+        "ring": dict(positions=ring_pts, volumes=rng.uniform(1e-4, 2e-4, 3000),
+                     args=(0.05, 1e-4, np.array([0.1, -0.05, 0.02]), 1.0, 1.0, 0.1, 0.02,
+                           0.3, 5.0)),
+        "ring_plain": dict(positions=ring_pts[:1000], volumes=np.full(1000, 1.5e-4),
+                           args=(0.04, 2e-5, np.zeros(3), 0.8, 2.0, 0.15)),
+        "lamb": dict(positions=rng.uniform(-0.5, 0.5, size=(2000, 3)),
+                     volumes=rng.uniform(1e-4, 2e-4, 2000),
+                     args=(0.05, 1e-4, np.array([0.02, -0.01, 0.0]), 1.5, 0.12, 0.01, 0.7,
+                           12.0)),
+        "rect3": dict(box=np.array([-1.0, 1.0, -0.5, 0.5, -0.3, 0.3]), spacing=0.1),
+        "rect3b": dict(box=np.array([-0.7, 0.9, -0.25, 0.55, 0.0, 0.4]), spacing=0.037),
+        "rect2": dict(box=np.array([-1.0, 1.0, -0.6, 0.4, 0.0, 0.0]), spacing=0.03),
+        "hex": dict(box=np.array([-0.5, 0.5, -0.4, 0.4, -0.2, 0.2]), spacing=0.05),
+        "cyl_x": dict(d=0.05, radius=1.0, height=2.0, center=np.zeros(3), axis="x"),
+        "cyl_y": dict(d=0.07, radius=0.6, height=1.3, center=np.array([0.1, 0.2, -0.3]),
+                      axis="y"),
+        "cyl_z": dict(d=0.09, radius=0.5, height=0.8, center=np.array([-1.0, 0.0, 2.0]),
+                      axis="z"),
+    }
+
+
+def make_ic(ref):
+    util = os.path.join(ref, "OpenONDA", "utilities")
+    fm = load_by_path("ref_vpm_flow_models", os.path.join(util, "vpm_flow_models.py"))
+    sh = load_by_path("ref_vpm_solver_helper", os.path.join(util, "vpm_solver_helper.py"))
+    out = {}
+    for name, c in ic_cases().items():
+        if name.startswith("ring") or name == "lamb":
+            fn = fm.vortex_ring_vpm if name.startswith("ring") else fm.lamb_oseen_vpm
+            vel, a, s, nu = fn(c["positions"], c["volumes"], *c["args"])
+            out[f"{name}/positions"] = c["positions"]
+            out[f"{name}/volumes"] = c["volumes"]
+            for k, v in (("velocities", vel), ("strengths", a), ("radii", s),
+                         ("viscosities", nu)):
+                out[f"{name}/{k}"] = v
+        elif name.startswith("rect"):
+            fn = (sh.get_rectangular_point_distribuition if name != "rect2"
+                  else sh.get_2D_rectangular_point_distribuition)
+            out[f"{name}/points"], out[f"{name}/volumes"] = fn(c["box"], c["spacing"])
+        elif name == "hex":
+            out[f"{name}/points"], out[f"{name}/volumes"] = sh.get_hexagonal_point_distribution(
+                c["box"], c["spacing"])
+        else:
+            out[f"{name}/points"], out[f"{name}/volumes"] = \
+                sh.get_cylindrical_point_distribuition(c["d"], c["radius"], c["height"],
+                                                        c["center"], c["axis"])
+    np.savez_compressed(os.path.join(HERE, "ic.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=DEFAULT_REF)
@@ -366,6 +424,7 @@ def main():
         "steps_cpu": make_steps_cpu,
         "steps_gpu": make_steps_gpu,
         "step_ring8192": make_step_ring8192,
+        "ic": make_ic,
     }
     only = set(args.only.split(",")) if args.only else set(jobs)
     for name, fn in jobs.items():
