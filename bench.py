@@ -208,22 +208,24 @@ class ClockSampler:
 # ----------------------------------------------------------------------------------------
 # B200 arm
 # ----------------------------------------------------------------------------------------
-def measure_fp32_peak(torch, kernels, dev):
+def measure_fp32_peak(torch, kernels, dev, kind=0, iters=1 << 15):
+    """Throughput of one pipe by microbenchmark: kind 0 = FP32 FFMA (returns TFLOP/s, FMA =
+    2 flops), kind 2 = MUFU rsqrt (returns T rsqrt/s)."""
     props = torch.cuda.get_device_properties(dev)
-    blocks, threads, iters = props.multi_processor_count * 8, 256, 1 << 15
+    blocks, threads = props.multi_processor_count * 8, 256
     sink = torch.empty(blocks * threads, dtype=torch.float32, device=dev)
-    kernels.launch_fma_peak(False, blocks, threads, 64, sink)
+    kernels.launch_fma_peak(kind, blocks, threads, 64, sink)
     best = None
     for _ in range(5):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        kernels.launch_fma_peak(False, blocks, threads, iters, sink)
+        kernels.launch_fma_peak(kind, blocks, threads, iters, sink)
         e1.record()
         e1.synchronize()
         t = e0.elapsed_time(e1) / 1e3
         best = t if best is None else min(best, t)
-    fmas = blocks * threads * iters * 16
-    return 2.0 * fmas / best / 1e12
+    ops = blocks * threads * iters * 16
+    return (2.0 if kind == 0 else 1.0) * ops / best / 1e12
 
 
 def load_traffic():
@@ -324,6 +326,7 @@ def main():
         return out
 
     peak = measure_fp32_peak(torch, kernels, dev)
+    sfu_peak = measure_fp32_peak(torch, kernels, dev, kind=2, iters=1 << 13)
     sampler = ClockSampler(local_rank) if rank == 0 else None
     t32, (u32, g32), clocks = timed(step32, args.steps, args.warmup, sampler)
     sweep_events = sweep_events[-args.steps:]
@@ -451,7 +454,14 @@ def main():
                          "peak_source": "FFMA microbenchmark measured in this run",
                          "flops_per_pair": FLOPS_PER_PAIR_FUSED,
                          "fp32_pipe_frac": round(achieved / peak * 2 * FP32_OPS_PER_PAIR_FUSED
-                                                 / FLOPS_PER_PAIR_FUSED, 4)},
+                                                 / FLOPS_PER_PAIR_FUSED, 4),
+                         "sfu": {"rsqrt_per_pair": 1,
+                                 "achieved_t_per_s": round(pairs_per_launch / t_sweep / 1e12,
+                                                           4),
+                                 "peak_t_per_s": round(sfu_peak, 4),
+                                 "frac": round(pairs_per_launch / t_sweep / 1e12 / sfu_peak,
+                                               4),
+                                 "peak_source": "MUFU rsqrt microbenchmark in this run"}},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "cpu_baseline": cpu,

@@ -56,7 +56,8 @@ enum vpm_op {
   VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS = 8,
   VPM_OP_RHS_VJP = 9,             /* adjoint of (velocity, stretching) */
   VPM_OP_RHS_VJP_PSE = 10,        /* adjoint of (velocity, stretching + PSE) */
-  VPM_OP_KINETIC_ENERGY_GRAD = 11 /* gradient of the kinetic energy */
+  VPM_OP_KINETIC_ENERGY_GRAD = 11, /* gradient of the kinetic energy */
+  VPM_OP_LES_STEP_SUMS = 12        /* velocity, stretching, vorticity, enstrophy in one sweep */
 };
 
 /* ---- library information ------------------------------------------------------------ */
@@ -136,6 +137,15 @@ int vpm_velocity_and_strength_gradients(const double* positions, const double* s
                                         const double* radii, int64_t n, double* velocities,
                                         double* dalpha_dt, int precision, void* workspace,
                                         size_t workspace_bytes, void* stream);
+
+/* The four pair sums of one dynamic-LES time step on the same state, in one sweep:
+ * get_selfinduced_velocity, get_strength_gradients, get_vorticity_field_at(positions, ...)
+ * and get_total_enstrophy (vpmModule.py:704, :753, :640, :644).  `enstrophy` is a device
+ * scalar; ref_extra_4pi as in vpm_total_enstrophy.  Workspace: VPM_OP_LES_STEP_SUMS. */
+int vpm_les_step_sums(const double* positions, const double* strengths, const double* radii,
+                      int64_t n, double* velocities, double* dalpha_dt, double* vorticity,
+                      double* enstrophy, int ref_extra_4pi, int precision, void* workspace,
+                      size_t workspace_bytes, void* stream);
 
 /* ---- adjoint (differentiation form; no counterpart in the reference) ------------------ */
 /* Vector-Jacobian product of the right-hand side F = (u, S [+ P]) of the coupled ODE
@@ -266,9 +276,10 @@ int vpm_selfinduced_velocity_noalloc(const double* positions, const double* stre
  * read from global memory, FP64 powers.  bench.py times it as the reference-algorithm GPU bar. */
 int vpm_naive_reference_kernel(int which, const double* positions, const double* strengths,
                                const double* radii, int64_t n, double* out, void* stream);
-/* FP32 FMA (fp64 != 0: FP64 FMA) throughput kernel: blocks x threads threads each run
- * `iters` iterations of 16 independent FMA chains; one value per thread lands in `sink`
- * (blocks*threads floats or doubles).  FMA count = blocks*threads*iters*16. */
+/* Pipe throughput kernels: blocks x threads threads each run `iters` iterations of 16
+ * independent chains; one value per thread lands in `sink` (blocks*threads floats, or doubles
+ * for FP64).  fp64 = 0: FP32 FMA, 1: FP64 FMA, 2: FP32 MUFU rsqrt (SFU).  Operation count =
+ * blocks*threads*iters*16. */
 int vpm_launch_fma_peak(int fp64, int blocks, int threads, int iters, void* sink, void* stream);
 
 #ifdef __cplusplus

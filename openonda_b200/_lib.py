@@ -34,6 +34,7 @@ OPS = {
     "rhs_vjp": 9,
     "rhs_vjp_pse": 10,
     "kinetic_energy_grad": 11,
+    "les_step_sums": 12,
 }
 
 _P = ctypes.c_void_p
@@ -61,6 +62,7 @@ SIGNATURES = {
     "vpm_total_helicity": ([_P, _P, _P, _I64, _I, _P, _I, _P, _SZ, _P], _I),
     "vpm_total_enstrophy": ([_P, _P, _P, _I64, _I, _P, _I, _P, _SZ, _P], _I),
     "vpm_velocity_and_strength_gradients": ([_P, _P, _P, _I64, _P, _P, _I, _P, _SZ, _P], _I),
+    "vpm_les_step_sums": ([_P, _P, _P, _I64, _P, _P, _P, _P, _I, _I, _P, _SZ, _P], _I),
     "vpm_rhs_vjp": ([_P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _I, _P, _SZ, _P], _I),
     "vpm_kinetic_energy_grad": ([_P, _P, _P, _I64, _P, _P, _P, _I, _P, _SZ, _P], _I),
     "vpm_record_bytes": ([_I], _SZ),

@@ -234,7 +234,8 @@ int pack(const double* pos, const double* str, const double* rad, const double* 
 }
 
 // ---- finalize kernels -----------------------------------------------------------------
-enum FinKind { FIN_VEL = 0, FIN_VORT = 1, FIN_STRETCH = 2, FIN_PSE = 3, FIN_VELSTRETCH = 4 };
+enum FinKind { FIN_VEL = 0, FIN_VORT = 1, FIN_STRETCH = 2, FIN_PSE = 3, FIN_VELSTRETCH = 4,
+               FIN_LES = 5 };
 
 template <int NV>
 __device__ __forceinline__ void sum_splits(const double* __restrict__ part, int splits, int64_t m,
@@ -251,7 +252,7 @@ __device__ __forceinline__ void sum_splits(const double* __restrict__ part, int 
 template <class T, int KIND, int NV>
 __global__ void finalize_vec_kernel(const double* __restrict__ part, int splits, int64_t m,
                                     const Rec<T>* __restrict__ tgt, double* __restrict__ out,
-                                    double* __restrict__ out2) {
+                                    double* __restrict__ out2, double* __restrict__ out3) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= m) return;
   double v[NV];
@@ -271,10 +272,17 @@ __global__ void finalize_vec_kernel(const double* __restrict__ part, int splits,
     out[3 * i + 1] = v[1] * c;
     out[3 * i + 2] = v[2] * c;
   } else {
-    constexpr int o = (KIND == FIN_VELSTRETCH) ? 3 : 0;
-    double* so = (KIND == FIN_VELSTRETCH) ? out2 : out;
+    constexpr bool kVel = (KIND == FIN_VELSTRETCH || KIND == FIN_LES);
+    constexpr int o = kVel ? 3 : 0;
+    double* so = kVel ? out2 : out;
     const double bx = elem(tgt[i].ax), by = elem(tgt[i].ay), bz = elem(tgt[i].az);
-    if constexpr (KIND == FIN_VELSTRETCH) {
+    if constexpr (KIND == FIN_LES) {
+      const double c = 7.5 * kOneOver4Pi;
+      out3[3 * i] = v[9] * c;
+      out3[3 * i + 1] = v[10] * c;
+      out3[3 * i + 2] = v[11] * c;
+    }
+    if constexpr (kVel) {
       out[3 * i] = -v[0] * kOneOver4Pi;
       out[3 * i + 1] = -v[1] * kOneOver4Pi;
       out[3 * i + 2] = -v[2] * kOneOver4Pi;
@@ -288,16 +296,21 @@ __global__ void finalize_vec_kernel(const double* __restrict__ part, int splits,
 
 constexpr int kReduceThreads = 1024;
 
-// Single-block, fixed-order reduction of  sign * a_i . V_i  over all targets.
-template <class T>
+// Single-block, fixed-order reduction of  scale * a_i . V_i  over all targets, V_i being
+// values OFF..OFF+2 of NV partial sums per target.
+template <class T, int NV = 3, int OFF = 0>
 __global__ void __launch_bounds__(kReduceThreads)
 finalize_dot_kernel(const double* __restrict__ part, int splits, int64_t m,
                     const Rec<T>* __restrict__ tgt, double scale, double* __restrict__ out) {
   __shared__ double red[kReduceThreads];
   double acc = 0.0;
   for (int64_t i = threadIdx.x; i < m; i += kReduceThreads) {
-    double v[3];
-    sum_splits<3>(part, splits, m, i, v);
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int s = 0; s < splits; ++s) {
+      const double* p = part + int64_t(s) * NV * m + int64_t(OFF) * m;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) v[k] += p[int64_t(k) * m + i];
+    }
     acc += elem(tgt[i].ax) * v[0] + elem(tgt[i].ay) * v[1] + elem(tgt[i].az) * v[2];
   }
   red[threadIdx.x] = acc;
@@ -313,11 +326,11 @@ __global__ void write_scalar_kernel(double* out, double v) { out[0] = v; }
 
 template <class T, int KIND, int NV>
 int finalize_vec(const double* part, int splits, int64_t m, const Rec<T>* tgt, double* out,
-                 double* out2, cudaStream_t st) {
+                 double* out2, cudaStream_t st, double* out3 = nullptr) {
   if (m <= 0) return VPM_OK;
   const int threads = 256;
-  finalize_vec_kernel<T, KIND, NV>
-      <<<unsigned((m + threads - 1) / threads), threads, 0, st>>>(part, splits, m, tgt, out, out2);
+  finalize_vec_kernel<T, KIND, NV><<<unsigned((m + threads - 1) / threads), threads, 0, st>>>(
+      part, splits, m, tgt, out, out2, out3);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "finalize launch");
   return VPM_OK;
@@ -428,6 +441,7 @@ struct Ops {
   using Ke = OpKe<T, REFINE>;
   using Ens = OpEns<T, REFINE>;
   using VelStretch = OpVelStretch<T, REFINE>;
+  using LesStep = OpLesStep<T, REFINE>;
   using RhsVjp = OpRhsVjp<T, REFINE, false>;
   using RhsVjpPse = OpRhsVjp<T, REFINE, true>;
   using KeGrad = OpKeGrad<T, REFINE>;
@@ -456,6 +470,8 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
       return Sweep<typename O::Ens, T>::plan(m, n, p, mpb);
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
       return Sweep<typename O::VelStretch, T>::plan(m, n, p, mpb);
+    case VPM_OP_LES_STEP_SUMS:
+      return Sweep<typename O::LesStep, T>::plan(m, n, p, mpb);
     case VPM_OP_RHS_VJP:
       return Sweep<typename O::RhsVjp, T>::plan(m, n, p, mpb);
     case VPM_OP_RHS_VJP_PSE:
@@ -516,6 +532,8 @@ struct Call {
   const void* records = nullptr;  // pre-packed sources (self sums); null = pack from AoS
   int64_t tgt_begin = 0;          // self sums: targets are records[tgt_begin, tgt_begin + m)
   size_t max_partial_bytes = kMaxPartialBytes;  // caps the source splits of the plan
+  double* out3 = nullptr;  // VPM_OP_LES_STEP_SUMS: vorticity (m,3)
+  double* out4 = nullptr;  // VPM_OP_LES_STEP_SUMS: enstrophy (device scalar)
 };
 
 template <class T, bool REFINE>
@@ -534,6 +552,8 @@ int run(const Call& c) {
     }
     rc = zero_out(c.out, 3 * (c.m > 0 ? c.m : 0), c.st);
     if (!rc && c.out2) rc = zero_out(c.out2, 3 * (c.m > 0 ? c.m : 0), c.st);
+    if (!rc && c.out3) rc = zero_out(c.out3, 3 * (c.m > 0 ? c.m : 0), c.st);
+    if (!rc && c.out4) rc = zero_out(c.out4, 1, c.st);
     return rc;
   }
 
@@ -590,6 +610,20 @@ int run(const Call& c) {
         rc = finalize_vec<T, FIN_VELSTRETCH, O::VelStretch::NV>(part, p.splits, c.m, tgt, c.out,
                                                                c.out2, c.st);
       return rc;
+    case VPM_OP_LES_STEP_SUMS: {
+      using Op = typename O::LesStep;
+      rc = Sweep<Op, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+      if (!rc)
+        rc = finalize_vec<T, FIN_LES, Op::NV>(part, p.splits, c.m, tgt, c.out, c.out2, c.st,
+                                               c.out3);
+      if (rc) return rc;
+      double scale = 1.0 / (8.0 * kPi);
+      if (c.ref_extra_4pi) scale /= 4.0 * kPi;
+      finalize_dot_kernel<T, Op::NV, 12><<<1, kReduceThreads, 0, c.st>>>(part, p.splits, c.m,
+                                                                          tgt, scale, c.out4);
+      cudaError_t e = cudaGetLastError();
+      return e == cudaSuccess ? VPM_OK : cuda_fail(e, "reduce launch");
+    }
     case VPM_OP_TOTAL_KINETIC_ENERGY:
     case VPM_OP_TOTAL_HELICITY:
     case VPM_OP_TOTAL_ENSTROPHY: {
@@ -633,8 +667,11 @@ int dispatch(const Call& c, int precision) {
   if (is_probe(c.op) && c.m > 0 && !c.tgt) return fail(VPM_ERR_ARG, "null targets pointer");
   if (c.op == VPM_OP_STRENGTH_GRADIENTS_PSE && c.n > 0 && !c.nu && !c.records)
     return fail(VPM_ERR_ARG, "null viscosities pointer");
-  if (c.op == VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS && c.m > 0 && !c.out2)
+  if ((c.op == VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS || c.op == VPM_OP_LES_STEP_SUMS) &&
+      c.m > 0 && !c.out2)
     return fail(VPM_ERR_ARG, "null second output pointer");
+  if (c.op == VPM_OP_LES_STEP_SUMS && ((c.m > 0 && !c.out3) || !c.out4))
+    return fail(VPM_ERR_ARG, "null vorticity or enstrophy pointer");
   switch (precision) {
     case VPM_FP64:
       return run<double, false>(c);
@@ -773,6 +810,22 @@ __global__ void fma_peak_kernel(int iters, T* sink) {
     for (int k = 0; k < 16; ++k) a[k] = fma(a[k], m, b);
   }
   T s = 0;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) s += a[k];
+  sink[int64_t(blockIdx.x) * blockDim.x + threadIdx.x] = s;
+}
+
+// MUFU (SFU) throughput: 16 independent chains of rsqrt.approx per thread; the one FADD per
+// step runs on the FMA pipe, which has 8x the lanes of the SFU, so the SFU bounds the loop.
+__global__ void rsqrt_peak_kernel(int iters, float* sink) {
+  float a[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) a[k] = 1.0f + 1e-3f * float(threadIdx.x) + float(k);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) a[k] = rsqrt_approx(a[k] + 0.5f);
+  }
+  float s = 0.f;
 #pragma unroll
   for (int k = 0; k < 16; ++k) s += a[k];
   sink[int64_t(blockIdx.x) * blockDim.x + threadIdx.x] = s;
@@ -955,6 +1008,18 @@ int vpm_velocity_and_strength_gradients(const double* positions, const double* s
   return dispatch(c, precision);
 }
 
+int vpm_les_step_sums(const double* positions, const double* strengths, const double* radii,
+                      int64_t n, double* velocities, double* dalpha_dt, double* vorticity,
+                      double* enstrophy, int ref_extra_4pi, int precision, void* workspace,
+                      size_t workspace_bytes, void* stream) {
+  Call c{VPM_OP_LES_STEP_SUMS, nullptr, n, positions, strengths, radii,
+         nullptr, n, velocities, dalpha_dt, ref_extra_4pi, workspace, workspace_bytes,
+         static_cast<cudaStream_t>(stream)};
+  c.out3 = vorticity;
+  c.out4 = enstrophy;
+  return dispatch(c, precision);
+}
+
 size_t vpm_record_bytes(int precision) {
   switch (precision) {
     case VPM_FP64:
@@ -1059,12 +1124,15 @@ int vpm_selftest_bounded_wait(int* timed_out, void* stream) {
 }
 
 int vpm_launch_fma_peak(int fp64, int blocks, int threads, int iters, void* sink, void* stream) {
-  if (blocks <= 0 || threads <= 0 || threads > 1024 || iters <= 0 || !sink)
+  if (blocks <= 0 || threads <= 0 || threads > 1024 || iters <= 0 || !sink || fp64 < 0 ||
+      fp64 > 2)
     return fail(VPM_ERR_ARG, "bad fma peak launch arguments");
   int rc = check_arch();
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (fp64)
+  if (fp64 == 2)
+    rsqrt_peak_kernel<<<blocks, threads, 0, st>>>(iters, static_cast<float*>(sink));
+  else if (fp64)
     fma_peak_kernel<double><<<blocks, threads, 0, st>>>(iters, static_cast<double*>(sink));
   else
     fma_peak_kernel<float><<<blocks, threads, 0, st>>>(iters, static_cast<float*>(sink));

@@ -32,6 +32,7 @@
 //   OpPse      get_strength_gradients_PSE_kernel    :478-530
 //   OpKe       get_total_kinetic_energy_kernel      :563-642
 //   OpEns      get_total_enstrophy_kernel_simple    :867-920
+//   OpLesStep  OpVelStretch + OpVortAt (particles as probes) + OpEns on one state
 //   (helicity, :673-750, is  -a_i . sum_j g (r x a_j), i.e. a by-product of OpVel)
 #pragma once
 
@@ -226,6 +227,69 @@ struct OpVelStretch : PairOpBase<V> {
     acc[6] = fma(h, rx, acc[6]);
     acc[7] = fma(h, ry, acc[7]);
     acc[8] = fma(h, rz, acc[8]);
+  }
+};
+
+// ---- LES step sweep: velocity + stretching + both dynamic-LES filter sums ------------------
+// The LES time step needs, on the same (x, alpha, sigma), the velocity and stretching
+// (vpmModule.py:704, :753), the particle vorticity (:640, get_vorticity_field_at with the
+// particles as probes: source core sigma_j, r^2 <= 1e-8 skipped) and the enstrophy filter sum
+// (:644, pair core, all pairs).  One sweep gives all 15 sums:
+//   U, A, B as OpVelStretch;  W += s_j^4 y_j^7 a_j  (y_j = (r^2 + s_j^2)^-1/2);
+//   E += (x + 2.2 s^2) y^3 a_j.
+// Per pair 58 FP32 lane-ops and 2 MUFU (counts beside the statements): 39 for velocity and
+// stretching (one more than OpVelStretch, since r^2 is formed on its own for the vorticity),
+// 13 for the vorticity (incl. the r^2 test), 6 for the enstrophy; three separate sweeps cost
+// 38 + ~20 + ~15.  15 sums per target do not fit four targets per thread in registers, so
+// this operator runs two (one packed lane).
+#ifndef VPM_LES_R
+#define VPM_LES_R 2
+#endif
+template <class V, bool REFINE>
+struct OpLesStep : PairOpBase<V> {
+  static constexpr int kR = VPM_LES_R;
+  static constexpr int NV = 15;
+  __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
+                                              const int64_t*, int64_t) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;  // 3
+    const V sg = fma(s.s, splat<V>(0.5), t.hs);                // 1
+    const V s2 = sg * sg;                                      // 1
+    const V r2 = fma(rx, rx, fma(ry, ry, rz * rz));            // 3
+    const V x = r2 + s2;                                       // 1
+    const V y = rsqrt_lane<REFINE>(x);
+    const V y2 = y * y;                                        // 1
+    const V y5 = (y2 * y2) * y;                                // 2
+    const V t1 = fma(splat<V>(1.5), s2, x);                    // 1
+    const V g = t1 * y5;                                       // 1
+    const V f = (t1 + s2) * (y5 * y2);                         // 3
+    const V cx = fma(ry, s.az, -(rz * s.ay));                  // 6
+    const V cy = fma(rz, s.ax, -(rx * s.az));
+    const V cz = fma(rx, s.ay, -(ry * s.ax));
+    acc[0] = fma(g, cx, acc[0]);                               // 3
+    acc[1] = fma(g, cy, acc[1]);
+    acc[2] = fma(g, cz, acc[2]);
+    acc[3] = fma(g, s.ax - t.ax, acc[3]);                      // 6
+    acc[4] = fma(g, s.ay - t.ay, acc[4]);
+    acc[5] = fma(g, s.az - t.az, acc[5]);
+    const V h = f * fma(t.ax, cx, fma(t.ay, cy, t.az * cz));   // 4
+    acc[6] = fma(h, rx, acc[6]);                               // 3
+    acc[7] = fma(h, ry, acc[7]);
+    acc[8] = fma(h, rz, acc[8]);
+    // vorticity filter sum (source core)
+    const V sj2 = s.s * s.s;                                   // 1
+    const V yv = rsqrt_lane<REFINE>(r2 + sj2);                 // 1
+    const V yv2 = yv * yv;                                     // 4
+    const V yv3 = yv2 * yv;
+    const V yv7 = (yv3 * yv3) * yv;
+    const V kv = keep_if_gt(r2, kRefEps, (sj2 * sj2) * yv7);   // 2 (+ compare/select)
+    acc[9] = fma(kv, s.ax, acc[9]);                            // 3
+    acc[10] = fma(kv, s.ay, acc[10]);
+    acc[11] = fma(kv, s.az, acc[11]);
+    // enstrophy filter sum (pair core)
+    const V ke = fma(splat<V>(2.2), s2, x) * (y2 * y);         // 3
+    acc[12] = fma(ke, s.ax, acc[12]);                          // 3
+    acc[13] = fma(ke, s.ay, acc[13]);
+    acc[14] = fma(ke, s.az, acc[14]);
   }
 };
 

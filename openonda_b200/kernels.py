@@ -132,6 +132,23 @@ def velocity_and_strength_gradients(positions, strengths, radii, precision="fp64
     return u, g
 
 
+def les_step_sums(positions, strengths, radii, ref_extra_4pi=True, precision="fp64"):
+    """Velocity, stretching, particle vorticity and the enstrophy filter sum of one
+    dynamic-LES step, from one sweep over the same state.  Returns (u, dalpha_dt, omega,
+    enstrophy) with the enstrophy as a 0-d tensor."""
+    x, a, s, n, dev = _self_inputs(positions, strengths, radii)
+    u = torch.empty((n, 3), dtype=_F64, device=dev)
+    g = torch.empty((n, 3), dtype=_F64, device=dev)
+    w = torch.empty((n, 3), dtype=_F64, device=dev)
+    e = torch.empty((), dtype=_F64, device=dev)
+    ws, nb = _workspace("les_step_sums", precision, n, n, dev)
+    _lib.check(_lib.load().vpm_les_step_sums(
+        _ptr(x), _ptr(a), _ptr(s), n, _ptr(u), _ptr(g), _ptr(w), _ptr(e),
+        int(bool(ref_extra_4pi)), _lib.precision_code(precision), _ptr(ws), ws.numel(),
+        _stream(dev)))
+    return u, g, w, e
+
+
 def strength_gradients_pse(positions, strengths, radii, viscosities, precision="fp64"):
     x, a, s, n, dev = _self_inputs(positions, strengths, radii)
     v = _check_scalar("viscosities", viscosities, n)
@@ -205,6 +222,7 @@ def device_errors(clear: bool = True) -> int:
     return v.value
 
 
-def launch_fma_peak(fp64: bool, blocks: int, threads: int, iters: int, sink: torch.Tensor):
+def launch_fma_peak(fp64, blocks: int, threads: int, iters: int, sink: torch.Tensor):
+    """fp64: False/0 = FP32 FMA, True/1 = FP64 FMA, 2 = FP32 MUFU rsqrt (SFU)."""
     _lib.check(_lib.load().vpm_launch_fma_peak(int(fp64), blocks, threads, iters,
                                                sink.data_ptr(), _stream(sink.device)))

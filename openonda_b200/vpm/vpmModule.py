@@ -12,8 +12,10 @@ step runs on the B200 library:
   spreading, dynamic-LES constant and sub-grid viscosity, relaxation) and the O(N) FP64
   diagnostics through the library's own kernels;
 * ``update_velocities`` evaluates velocity and stretching in one fused sweep when the flow
-  model needs stretching; ``update_strengths`` reuses that rate while the state is unchanged
-  (the reference evaluates both on the same positions/strengths, vpmModule.py:704,753-774).
+  model needs stretching (for LES the same sweep also gives the particle vorticity and the
+  enstrophy filter sum); ``update_strengths`` reuses those sums while the state is unchanged
+  (the reference evaluates them all on the same positions/strengths, vpmModule.py:640,644,
+  704,753-774).
 
 Reference behaviours kept: Euler/BDF2/BDF3/BDF4 ladder by ``time_step`` with the history
 rewritten after stretching and again after PSE; RK stage 1 reuses the velocities of
@@ -144,6 +146,8 @@ class ParticleSystem:
         self._cnu_host = CNU_0
         self._rate = None  # stretching rate from the fused sweep, valid for self._rate_token
         self._rate_token = None
+        self._les_w = None  # LES vorticity / enstrophy from the same sweep (same token)
+        self._les_ens = None
         self._token = 0
 
     # ---- validation (vpmModule.py:158-184) ------------------------------------------
@@ -604,7 +608,12 @@ class ParticleSystem:
         the same sweep also yields the stretching rate for update_strengths."""
         if self._n == 0:
             return
-        if self.flow_model in ("LES", "DNS"):
+        if self.flow_model == "LES":
+            # one sweep also yields the two LES filter sums update_strengths needs next
+            self._u, self._rate, self._les_w, self._les_ens = kernels.les_step_sums(
+                self._x, self._a, self._s, ref_extra_4pi=True, precision=self.precision)
+            self._rate_token = self._token
+        elif self.flow_model == "DNS":
             self._u, self._rate = kernels.velocity_and_strength_gradients(
                 self._x, self._a, self._s, precision=self.precision)
             self._rate_token = self._token
@@ -638,9 +647,13 @@ class ParticleSystem:
             return
         dev = self._dev()
         if self.flow_model == "LES":
-            w = self._vorticity()
-            ens = kernels.total_enstrophy(self._x, self._a, self._s, ref_extra_4pi=True,
-                                          precision=self.precision)
+            if self._les_w is not None and self._rate_token == self._token:
+                w, ens = self._les_w, self._les_ens
+            else:
+                w = self._vorticity()
+                ens = kernels.total_enstrophy(self._x, self._a, self._s, ref_extra_4pi=True,
+                                              precision=self.precision)
+            self._les_w = self._les_ens = None
             self._les_update(w, ens)
         rate_s = None
         if self.flow_model in ("LES", "DNS"):

@@ -240,6 +240,38 @@ def config5(args):
            "cnu": ps.Cnu})
 
 
+def sweeps(args):
+    """Time of each FP32c sweep of an LES step on the dynamic-LES ring (default N = 2^20):
+    the fused LES step sums against the separate sweeps they replace, plus PSE and the
+    velocity-only RK-stage sweep."""
+    n = args.n or (1 << 20)
+    k = 1 << (int(np.log2(n)) // 2)
+    f = configs.les_ring(n_azimuthal=k, n_section=n // k)
+    n = f.n
+    r = lambda z: torch.from_numpy(np.asarray(z, np.float64)).cuda()
+    x, a, s, nu = r(f.positions), r(f.strengths), r(f.radii), r(f.viscosities)
+    p = "fp32c"
+    cases = {
+        "les_step_sums": lambda: kernels.les_step_sums(x, a, s, precision=p),
+        "velocity_and_strength_gradients":
+            lambda: kernels.velocity_and_strength_gradients(x, a, s, precision=p),
+        "vorticity_field_at": lambda: kernels.vorticity_field_at(x, x, a, s, precision=p),
+        "total_enstrophy": lambda: kernels.total_enstrophy(x, a, s, precision=p),
+        "strength_gradients_pse":
+            lambda: kernels.strength_gradients_pse(x, a, s, nu, precision=p),
+        "selfinduced_velocity": lambda: kernels.selfinduced_velocity(x, a, s, precision=p),
+    }
+    reps = args.steps or 3
+    for name, fn in cases.items():
+        fn()
+        with _Timer() as t:
+            for _ in range(reps):
+                fn()
+        ms = t.ms / reps
+        _emit({"sweep": name, "n": n, "precision": p, "ms": round(ms, 2),
+               "gpairs_per_s": round(float(n) * n / (ms / 1e3) / 1e9, 1)})
+
+
 def stepkernels(args):
     from . import _lib
 
@@ -278,7 +310,7 @@ def stepkernels(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("workload", choices=["config1", "config2", "config3", "config4", "config5",
-                                         "stepkernels"])
+                                         "stepkernels", "sweeps"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--fd", type=int, default=None)
     ap.add_argument("--n", type=int, default=None)

@@ -1,0 +1,93 @@
+"""Parity at the headline size, N = 2^20 (the random cloud of the throughput sweep at 1M).
+
+The full FP64 sum is too large for the oracle, so it checks windows of targets against all
+2^20 sources (oracle ``*_range`` functions, the reference's GPU semantics): rows at the
+start, in the middle and at the end of the target range, i.e. in different target blocks and
+on both sides of block boundaries.  Around that, size-independent properties: the FP32c
+path against the FP64 path on the whole field, exact scaling under alpha -> 2 alpha
+(velocity and PSE are linear in alpha, stretching quadratic; scaling by 2 is exact in both
+precisions, so the results must be bitwise), and bitwise repeatability."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import normwise
+
+pytestmark = pytest.mark.gpu
+
+N = 1 << 20
+WINDOWS = [(0, 192), (N // 2 - 96, N // 2 + 96), (N - 192, N)]
+# Each result is a sum of 2^20 FP64 terms that largely cancel (stretching: a_i x sum g
+# (a_j - a_i) + 3 sum f (...) r); the oracle sums sources in index order, the kernel per
+# split and tile, so the two differ by the rounding of a 2^20-term sum times its condition
+# (~1e-12 measured for the stretching).  The 1e-12 bar of the 8192-particle ring
+# (test_parity_gpu) holds there at ~1e-16.
+FP64_TOL_2_20 = 1e-11
+
+
+@pytest.fixture(scope="module")
+def cloud():
+    from openonda_b200 import configs
+
+    f = configs.random_cloud(N, seed=0)
+    t = lambda z: torch.from_numpy(np.ascontiguousarray(z)).cuda()
+    return f, t(f.positions), t(f.strengths), t(f.radii), t(f.viscosities)
+
+
+@pytest.fixture(scope="module")
+def fp64(cloud):
+    from openonda_b200 import kernels
+
+    _, x, a, s, _ = cloud
+    return kernels.velocity_and_strength_gradients(x, a, s, precision="fp64")
+
+
+def test_fp64_windows_vs_oracle(cloud, fp64):
+    f = cloud[0]
+    u, g = fp64[0].cpu().numpy(), fp64[1].cpu().numpy()
+    for t0, t1 in WINDOWS:
+        ru = oracle.gpu.selfinduced_velocity_range(f.positions, f.strengths, f.radii, t0, t1)
+        rg = oracle.gpu.strength_gradients_range(f.positions, f.strengths, f.radii, t0, t1)
+        eu, eg = normwise(u[t0:t1], ru), normwise(g[t0:t1], rg)
+        print(f"window [{t0}, {t1}): velocity {eu:.2e}, stretching {eg:.2e}")
+        assert eu <= FP64_TOL_2_20, (t0, eu)
+        assert eg <= FP64_TOL_2_20, (t0, eg)
+
+
+def test_fp32c_vs_fp64_full_size(cloud):
+    from openonda_b200 import kernels
+
+    _, x, a, s, _ = cloud
+    r32 = lambda z: z.float().double()
+    x, a, s = r32(x), r32(a), r32(s)
+    u64, g64 = kernels.velocity_and_strength_gradients(x, a, s, precision="fp64")
+    u32, g32 = kernels.velocity_and_strength_gradients(x, a, s, precision="fp32c")
+    eu = float((u32 - u64).abs().max() / u64.abs().max())
+    eg = float((g32 - g64).abs().max() / g64.abs().max())
+    print(f"N=2^20 fp32c vs fp64: velocity {eu:.2e}, stretching {eg:.2e}")
+    assert eu <= 1e-6
+    assert eg <= 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_exact_scaling_in_alpha(cloud, precision):
+    from openonda_b200 import kernels
+
+    _, x, a, s, nu = cloud
+    u1, g1 = kernels.velocity_and_strength_gradients(x, a, s, precision=precision)
+    u2, g2 = kernels.velocity_and_strength_gradients(x, 2.0 * a, s, precision=precision)
+    assert torch.equal(u2, 2.0 * u1)
+    assert torch.equal(g2, 4.0 * g1)
+    p1 = kernels.strength_gradients_pse(x, a, s, nu, precision=precision)
+    p2 = kernels.strength_gradients_pse(x, 2.0 * a, s, nu, precision=precision)
+    assert torch.equal(p2, 2.0 * p1)
+
+
+def test_full_size_repeatable(cloud, fp64):
+    from openonda_b200 import kernels
+
+    _, x, a, s, _ = cloud
+    u, g = kernels.velocity_and_strength_gradients(x, a, s, precision="fp64")
+    assert torch.equal(u, fp64[0]) and torch.equal(g, fp64[1])
+    assert kernels.device_errors() == 0

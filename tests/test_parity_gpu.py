@@ -283,3 +283,49 @@ def test_naive_reference_kernels_match_oracle():
         _lib.check(lib.vpm_naive_reference_kernel(which, x.data_ptr(), a.data_ptr(),
                                                   s.data_ptr(), 1500, out.data_ptr(), st))
         assert normwise(out.cpu().numpy(), ref(f.positions, f.strengths, f.radii)) <= 1e-13
+
+
+@pytest.mark.parametrize("n", [1, 97, 2048, 5000])
+def test_les_step_sums_vs_oracle(n):
+    """One sweep = get_selfinduced_velocity + get_strength_gradients +
+    get_vorticity_field_at(x, x, ...) + get_total_enstrophy (reference GPU semantics)."""
+    import torch
+
+    from openonda_b200 import configs, kernels
+
+    f = configs.random_cloud(n, seed=n)
+    f.radii *= 4
+    x, a, s = (torch.from_numpy(np.ascontiguousarray(z)).cuda()
+               for z in (f.positions, f.strengths, f.radii))
+    u, g, w, e = kernels.les_step_sums(x, a, s, ref_extra_4pi=True, precision="fp64")
+    o = oracle.gpu
+    assert normwise(u.cpu().numpy(), o.get_selfinduced_velocity(f.positions, f.strengths,
+                                                                f.radii)) <= FP64_TOL
+    assert normwise(g.cpu().numpy(), o.get_strength_gradients(f.positions, f.strengths,
+                                                              f.radii)) <= FP64_TOL
+    assert normwise(w.cpu().numpy(), o.get_vorticity_field_at(f.positions, f.positions,
+                                                              f.strengths, f.radii)) <= FP64_TOL
+    ref_e = o.get_total_enstrophy(f.positions, f.strengths, f.radii)
+    assert abs(float(e) - ref_e) <= 1e-12 * abs(ref_e)
+    # FP32-compensated against FP64 on the same FP32-rounded inputs
+    r32 = lambda z: z.float().double()
+    x, a, s = r32(x), r32(a), r32(s)
+    ref = kernels.les_step_sums(x, a, s, precision="fp64")
+    got = kernels.les_step_sums(x, a, s, precision="fp32c")
+    for k, tol in zip(range(3), (FP32C_TOL, FP32C_STRETCH_TOL, FP32C_TOL)):
+        assert normwise(got[k].cpu().numpy(), ref[k].cpu().numpy()) <= tol, k
+    assert abs(float(got[3]) - float(ref[3])) <= FP32C_TOL * abs(float(ref[3]))
+
+
+def test_les_step_sums_empty_and_errors():
+    import torch
+
+    from openonda_b200 import _lib, kernels
+
+    z = torch.zeros((0, 3), dtype=torch.float64, device="cuda")
+    u, g, w, e = kernels.les_step_sums(z, z, torch.zeros(0, dtype=torch.float64,
+                                                         device="cuda"))
+    assert u.shape == (0, 3) and float(e) == 0.0
+    lib = _lib.load()
+    assert lib.vpm_les_step_sums(None, None, None, 4, None, None, None, None, 1, 0, None, 0,
+                                 None) == _lib.VPM_ERR_ARG
