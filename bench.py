@@ -209,8 +209,8 @@ class ClockSampler:
 # B200 arm
 # ----------------------------------------------------------------------------------------
 def measure_fp32_peak(torch, kernels, dev, kind=0, iters=1 << 15):
-    """Throughput of one pipe by microbenchmark: kind 0 = FP32 FFMA (returns TFLOP/s, FMA =
-    2 flops), kind 2 = MUFU rsqrt (returns T rsqrt/s)."""
+    """Throughput of one pipe by microbenchmark: kind 0 = FP32 FFMA, 3 = packed FFMA2 (both
+    in TFLOP/s, a lane FMA = 2 flops), kind 2 = MUFU rsqrt (T rsqrt/s)."""
     props = torch.cuda.get_device_properties(dev)
     blocks, threads = props.multi_processor_count * 8, 256
     sink = torch.empty(blocks * threads, dtype=torch.float32, device=dev)
@@ -225,7 +225,7 @@ def measure_fp32_peak(torch, kernels, dev, kind=0, iters=1 << 15):
         t = e0.elapsed_time(e1) / 1e3
         best = t if best is None else min(best, t)
     ops = blocks * threads * iters * 16
-    return (2.0 if kind == 0 else 1.0) * ops / best / 1e12
+    return {0: 2.0, 2: 1.0, 3: 4.0}[kind] * ops / best / 1e12
 
 
 def load_traffic():
@@ -327,6 +327,7 @@ def main():
 
     peak = measure_fp32_peak(torch, kernels, dev)
     sfu_peak = measure_fp32_peak(torch, kernels, dev, kind=2, iters=1 << 13)
+    ffma2_peak = measure_fp32_peak(torch, kernels, dev, kind=3, iters=1 << 14)
     sampler = ClockSampler(local_rank) if rank == 0 else None
     t32, (u32, g32), clocks = timed(step32, args.steps, args.warmup, sampler)
     sweep_events = sweep_events[-args.steps:]
@@ -455,6 +456,7 @@ def main():
                          "flops_per_pair": FLOPS_PER_PAIR_FUSED,
                          "fp32_pipe_frac": round(achieved / peak * 2 * FP32_OPS_PER_PAIR_FUSED
                                                  / FLOPS_PER_PAIR_FUSED, 4),
+                         "packed_ffma2_peak": round(ffma2_peak, 3),
                          "sfu": {"rsqrt_per_pair": 1,
                                  "achieved_t_per_s": round(pairs_per_launch / t_sweep / 1e12,
                                                            4),

@@ -278,8 +278,9 @@ int vpm_naive_reference_kernel(int which, const double* positions, const double*
                                const double* radii, int64_t n, double* out, void* stream);
 /* Pipe throughput kernels: blocks x threads threads each run `iters` iterations of 16
  * independent chains; one value per thread lands in `sink` (blocks*threads floats, or doubles
- * for FP64).  fp64 = 0: FP32 FMA, 1: FP64 FMA, 2: FP32 MUFU rsqrt (SFU).  Operation count =
- * blocks*threads*iters*16. */
+ * for FP64).  fp64 = 0: FP32 FMA, 1: FP64 FMA, 2: FP32 MUFU rsqrt (SFU), 3: packed FP32x2
+ * FMA (FFMA2), 4: 8 FFMA2 + 16 FFMA chains.  Operation count = blocks*threads*iters*16 (lane
+ * FMAs: twice that for 3 and 4). */
 int vpm_launch_fma_peak(int fp64, int blocks, int threads, int iters, void* sink, void* stream);
 
 #ifdef __cplusplus

@@ -815,6 +815,48 @@ __global__ void fma_peak_kernel(int iters, T* sink) {
   sink[int64_t(blockIdx.x) * blockDim.x + threadIdx.x] = s;
 }
 
+// Packed FP32 FMA throughput: 16 independent chains of FFMA2 (two FP32 lanes each).
+__global__ void ffma2_peak_kernel(int iters, float* sink) {
+  float2 a[16];
+  const float2 m = make_float2(1.0f - 1e-7f * float(threadIdx.x & 7), 1.0f - 2e-7f);
+  const float2 b = make_float2(1e-9f * float(blockIdx.x & 3), 1e-9f);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) a[k] = make_float2(float(threadIdx.x + k), float(k));
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) a[k] = fma(a[k], m, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) s += a[k].x + a[k].y;
+  sink[int64_t(blockIdx.x) * blockDim.x + threadIdx.x] = s;
+}
+
+// Mixed FP32 FMA throughput: 8 packed FFMA2 chains and 16 scalar FFMA chains per thread (32
+// lane FMAs per iteration in 24 instructions).
+__global__ void ffma_mixed_peak_kernel(int iters, float* sink) {
+  float2 a[8];
+  float c[16];
+  const float2 m = make_float2(1.0f - 1e-7f * float(threadIdx.x & 7), 1.0f - 2e-7f);
+  const float2 b = make_float2(1e-9f * float(blockIdx.x & 3), 1e-9f);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = make_float2(float(threadIdx.x + k), float(k));
+#pragma unroll
+  for (int k = 0; k < 16; ++k) c[k] = float(threadIdx.x + 2 * k);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      a[k] = fma(a[k], m, b);
+      c[2 * k] = fmaf(c[2 * k], m.x, b.x);
+      c[2 * k + 1] = fmaf(c[2 * k + 1], m.y, b.y);
+    }
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += a[k].x + a[k].y + c[2 * k] + c[2 * k + 1];
+  sink[int64_t(blockIdx.x) * blockDim.x + threadIdx.x] = s;
+}
+
 // MUFU (SFU) throughput: 16 independent chains of rsqrt.approx per thread; the one FADD per
 // step runs on the FMA pipe, which has 8x the lanes of the SFU, so the SFU bounds the loop.
 __global__ void rsqrt_peak_kernel(int iters, float* sink) {
@@ -1125,12 +1167,16 @@ int vpm_selftest_bounded_wait(int* timed_out, void* stream) {
 
 int vpm_launch_fma_peak(int fp64, int blocks, int threads, int iters, void* sink, void* stream) {
   if (blocks <= 0 || threads <= 0 || threads > 1024 || iters <= 0 || !sink || fp64 < 0 ||
-      fp64 > 2)
+      fp64 > 4)
     return fail(VPM_ERR_ARG, "bad fma peak launch arguments");
   int rc = check_arch();
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (fp64 == 2)
+  if (fp64 == 4)
+    ffma_mixed_peak_kernel<<<blocks, threads, 0, st>>>(iters, static_cast<float*>(sink));
+  else if (fp64 == 3)
+    ffma2_peak_kernel<<<blocks, threads, 0, st>>>(iters, static_cast<float*>(sink));
+  else if (fp64 == 2)
     rsqrt_peak_kernel<<<blocks, threads, 0, st>>>(iters, static_cast<float*>(sink));
   else if (fp64)
     fma_peak_kernel<double><<<blocks, threads, 0, st>>>(iters, static_cast<double*>(sink));

@@ -223,6 +223,7 @@ def device_errors(clear: bool = True) -> int:
 
 
 def launch_fma_peak(fp64, blocks: int, threads: int, iters: int, sink: torch.Tensor):
-    """fp64: False/0 = FP32 FMA, True/1 = FP64 FMA, 2 = FP32 MUFU rsqrt (SFU)."""
+    """fp64: False/0 = FP32 FMA, True/1 = FP64 FMA, 2 = FP32 MUFU rsqrt (SFU),
+    3 = packed FP32x2 FMA (FFMA2)."""
     _lib.check(_lib.load().vpm_launch_fma_peak(int(fp64), blocks, threads, iters,
                                                sink.data_ptr(), _stream(sink.device)))

@@ -16,6 +16,7 @@ config4  differentiation: perturbed ring N=65536, FP32c, loss = FP64-summed kine
 config5  dynamic-LES ring N=2^20, FP32c, PSE, RK4 dt=0.002: time per step, Gpairs/s, error vs
          FP64 at the last step.
 stepkernels  GB/s of the element-wise step kernels (RK stage, RK4 combine, BDF) at N=2^22.
+sweeps       time of each FP32c sweep of an LES step (fused LES sums vs the sweeps they replace).
 
 All inputs are the seeded synthetic fields of :mod:`openonda_b200.configs`.
 """
@@ -24,6 +25,8 @@ from __future__ import annotations
 import argparse
 import json
 import math
+import os
+import tempfile
 import time
 
 import numpy as np
@@ -61,7 +64,9 @@ class _Timer:
 def _system(field, precision, **kw):
     from .vpm.vpmModule import ParticleSystem
 
+    # the reference backs up at time step 0 (0 % frequency == 0): keep that file out of cwd
     ps = ParticleSystem(monitor_variables=[], backup_frequency=10 ** 9, precision=precision,
+                        backup_filename=os.path.join(tempfile.gettempdir(), "vpm_workload"),
                         **kw)
     ps.add_particle_field(field.positions, np.zeros_like(field.positions), field.strengths,
                           field.radii, field.viscosities)
@@ -90,9 +95,20 @@ def config1(args):
     so = StepOracle(oracle.gpu, f.positions, f.strengths, f.radii, f.viscosities, **kw)
     so.step()
     t_cpu = time.perf_counter() - t0
+    # steady state (time step >= 3): the eager loop against advance() with the CUDA graph
+    steady = {}
+    for mode in ("eager", "graph"):
+        sp = _system(f, "fp64", **kw)
+        sp.advance(4, use_graph=(mode == "graph"))  # BDF start-up (+ capture)
+        k = args.steps or 50
+        with _Timer() as tt:
+            sp.advance(k, use_graph=(mode == "graph"))
+        steady[mode] = round(tt.ms / k, 3)
     n = f.n
     _emit({"config": "config1", "workload": f.description, "n": n,
            "b200_ms_per_step": round(t.ms, 3), "sweeps_per_step": 5,
+           "steady_ms_per_step_eager": steady["eager"],
+           "steady_ms_per_step_cuda_graph": steady["graph"],
            "oracle_cpu_s_per_step": round(t_cpu, 2), "oracle_threads": oracle.num_threads(),
            "rel_err_positions": _rel(torch.from_numpy(ps.get_particle_positions()),
                                      torch.from_numpy(so.x)),
