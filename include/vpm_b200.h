@@ -43,6 +43,13 @@ enum vpm_status {
 };
 
 enum vpm_precision { VPM_FP64 = 0, VPM_FP32C = 1, VPM_FP32C_REFINED = 2 };
+/* Flag OR-ed into `precision` (self sums, records and workspace queries): the caller
+ * guarantees that every particle has the same core radius, so the pair core
+ * (sigma_i + sigma_j)/2 is sigma_i and the kernels skip forming it (2 FP32 operations fewer
+ * per pair, same values).  The pack step checks the claim and sets bit 1 of the device error
+ * word when a radius differs from radii[0] (results are then wrong).  Probe sums, the kinetic
+ * energy and the adjoint ignore the flag.  No counterpart in the reference. */
+#define VPM_UNIFORM_CORE 0x100
 
 enum vpm_op {
   VPM_OP_SELFINDUCED_VELOCITY = 0,
@@ -65,7 +72,8 @@ int vpm_abi_version(void);
 const char* vpm_last_error(void);
 /* Check that the current device is sm_100 (B200); VPM_ERR_ARCH otherwise. */
 int vpm_check_device(void);
-/* Read (and optionally clear) the device error word: bit 0 = a bounded wait timed out. */
+/* Read (and optionally clear) the device error word: bit 0 = a bounded wait timed out,
+ * bit 1 = VPM_UNIFORM_CORE was passed for radii that are not all equal. */
 int vpm_device_errors(int* out, int clear);
 /* Failure-detection self-test: one block waits on an mbarrier phase that never completes; the
  * bounded wait gives up after ~1 s, sets bit 0 of the device error word, writes 1 to the

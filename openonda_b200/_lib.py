@@ -127,8 +127,12 @@ def check(rc: int) -> None:
         raise VPMError(rc, msg.decode() if msg else "")
 
 
-def precision_code(precision: str) -> int:
+UNIFORM_CORE = 0x100  # VPM_UNIFORM_CORE: every particle has the same core radius
+
+
+def precision_code(precision: str, uniform_core: bool = False) -> int:
     try:
-        return PRECISIONS[precision]
+        code = PRECISIONS[precision]
     except KeyError:
         raise ValueError(f"unknown precision {precision!r}; choose from {sorted(PRECISIONS)}")
+    return code | (UNIFORM_CORE if uniform_core else 0)

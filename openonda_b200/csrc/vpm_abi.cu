@@ -206,9 +206,10 @@ __global__ void pack_particles_kernel(const double* __restrict__ pos,
                                       const double* __restrict__ str,
                                       const double* __restrict__ rad,
                                       const double* __restrict__ nu, int64_t n,
-                                      Rec<E>* __restrict__ out) {
+                                      Rec<E>* __restrict__ out, int check_uniform) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (check_uniform && rad[i] != rad[0]) atomicOr(&g_device_errors, VPM_DEVERR_NONUNIFORM_CORE);
   Rec<E> r;
   set_elem(r.x, pos[3 * i]);
   set_elem(r.y, pos[3 * i + 1]);
@@ -223,11 +224,12 @@ __global__ void pack_particles_kernel(const double* __restrict__ pos,
 
 template <class T>
 int pack(const double* pos, const double* str, const double* rad, const double* nu, int64_t n,
-         Rec<T>* out, cudaStream_t st) {
+         Rec<T>* out, cudaStream_t st, bool check_uniform = false) {
   if (n <= 0) return VPM_OK;
   const int threads = 256;
   const int64_t blocks = (n + threads - 1) / threads;
-  pack_particles_kernel<T><<<unsigned(blocks), threads, 0, st>>>(pos, str, rad, nu, n, out);
+  pack_particles_kernel<T><<<unsigned(blocks), threads, 0, st>>>(pos, str, rad, nu, n, out,
+                                                                 int(check_uniform && rad));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "pack launch");
   return VPM_OK;
@@ -431,17 +433,19 @@ __global__ void finalize_kegrad_kernel(const double* __restrict__ part, int spli
 }
 
 // ---- operator selection -----------------------------------------------------------------
-template <class T, bool REFINE>
+// UC: all cores equal (VPM_UNIFORM_CORE); the probe sums and the kinetic energy keep the
+// general form.
+template <class T, bool REFINE, bool UC = false>
 struct Ops {
-  using Vel = OpVel<T, REFINE>;
+  using Vel = OpVel<T, REFINE, UC>;
   using VelAt = OpVelAt<T, REFINE>;
   using VortAt = OpVortAt<T, REFINE>;
-  using Stretch = OpStretch<T, REFINE>;
-  using Pse = OpPse<T, REFINE>;
+  using Stretch = OpStretch<T, REFINE, UC>;
+  using Pse = OpPse<T, REFINE, UC>;
   using Ke = OpKe<T, REFINE>;
-  using Ens = OpEns<T, REFINE>;
-  using VelStretch = OpVelStretch<T, REFINE>;
-  using LesStep = OpLesStep<T, REFINE>;
+  using Ens = OpEns<T, REFINE, UC>;
+  using VelStretch = OpVelStretch<T, REFINE, UC>;
+  using LesStep = OpLesStep<T, REFINE, UC>;
   using RhsVjp = OpRhsVjp<T, REFINE, false>;
   using RhsVjpPse = OpRhsVjp<T, REFINE, true>;
   using KeGrad = OpKeGrad<T, REFINE>;
@@ -449,9 +453,9 @@ struct Ops {
 
 bool is_probe(int op) { return op == VPM_OP_INDUCED_VELOCITY_AT || op == VPM_OP_VORTICITY_FIELD_AT; }
 
-template <class T, bool REFINE>
+template <class T, bool REFINE, bool UC = false>
 int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes) {
-  using O = Ops<T, REFINE>;
+  using O = Ops<T, REFINE, UC>;
   switch (op) {
     case VPM_OP_SELFINDUCED_VELOCITY:
     case VPM_OP_TOTAL_HELICITY:
@@ -505,10 +509,10 @@ Layout layout_for(int op, const Plan& p, int64_t m, int64_t n) {
   return L;
 }
 
-template <class T, bool REFINE>
+template <class T, bool REFINE, bool UC = false>
 int workspace_for(int op, int64_t m, int64_t n, Layout* L, Plan* p,
                   size_t max_partial_bytes = kMaxPartialBytes) {
-  int rc = plan_op<T, REFINE>(op, m, n, p, max_partial_bytes);
+  int rc = plan_op<T, REFINE, UC>(op, m, n, p, max_partial_bytes);
   if (rc) return rc;
   *L = layout_for<T>(op, *p, m, n);
   return VPM_OK;
@@ -536,9 +540,9 @@ struct Call {
   double* out4 = nullptr;  // VPM_OP_LES_STEP_SUMS: enstrophy (device scalar)
 };
 
-template <class T, bool REFINE>
+template <class T, bool REFINE, bool UC>
 int run(const Call& c) {
-  using O = Ops<T, REFINE>;
+  using O = Ops<T, REFINE, UC>;
   int rc = check_arch();
   if (rc) return rc;
   const bool scalar = c.op == VPM_OP_TOTAL_KINETIC_ENERGY || c.op == VPM_OP_TOTAL_HELICITY ||
@@ -559,7 +563,7 @@ int run(const Call& c) {
 
   Plan p;
   Layout L;
-  rc = workspace_for<T, REFINE>(c.op, c.m, c.n, &L, &p, c.max_partial_bytes);
+  rc = workspace_for<T, REFINE, UC>(c.op, c.m, c.n, &L, &p, c.max_partial_bytes);
   if (rc) return rc;
   if (c.ws == nullptr) return fail(VPM_ERR_WORKSPACE, "workspace is null");
   if (reinterpret_cast<uintptr_t>(c.ws) % kAlign != 0)
@@ -574,7 +578,7 @@ int run(const Call& c) {
   double* part = reinterpret_cast<double*>(ws + L.part_off);
 
   if (!c.records) {
-    rc = pack<T>(c.pos, c.str, c.rad, c.nu, c.n, src, c.st);
+    rc = pack<T>(c.pos, c.str, c.rad, c.nu, c.n, src, c.st, UC);
     if (rc) return rc;
   }
   if (is_probe(c.op)) {
@@ -651,6 +655,28 @@ int run(const Call& c) {
   }
 }
 
+// Decoded precision code: compute type, Newton-refined rsqrt, uniform cores.
+template <class T, bool REFINE, bool UC>
+struct Prec {
+  using type = T;
+  static constexpr bool refine = REFINE, uc = UC;
+};
+
+template <class F>
+int with_precision(int precision, F&& f) {
+  const bool uc = (precision & VPM_UNIFORM_CORE) != 0;
+  switch (precision & ~VPM_UNIFORM_CORE) {
+    case VPM_FP64:
+      return uc ? f(Prec<double, false, true>{}) : f(Prec<double, false, false>{});
+    case VPM_FP32C:
+      return uc ? f(Prec<float2, false, true>{}) : f(Prec<float2, false, false>{});
+    case VPM_FP32C_REFINED:
+      return uc ? f(Prec<float2, true, true>{}) : f(Prec<float2, true, false>{});
+    default:
+      return fail(VPM_ERR_ARG, "unknown precision " + std::to_string(precision));
+  }
+}
+
 int dispatch(const Call& c, int precision) {
   if (c.n < 0 || c.m < 0) return fail(VPM_ERR_ARG, "negative size");
   if (c.records) {
@@ -672,16 +698,10 @@ int dispatch(const Call& c, int precision) {
     return fail(VPM_ERR_ARG, "null second output pointer");
   if (c.op == VPM_OP_LES_STEP_SUMS && ((c.m > 0 && !c.out3) || !c.out4))
     return fail(VPM_ERR_ARG, "null vorticity or enstrophy pointer");
-  switch (precision) {
-    case VPM_FP64:
-      return run<double, false>(c);
-    case VPM_FP32C:
-      return run<float2, false>(c);
-    case VPM_FP32C_REFINED:
-      return run<float2, true>(c);
-    default:
-      return fail(VPM_ERR_ARG, "unknown precision " + std::to_string(precision));
-  }
+  return with_precision(precision, [&](auto P) {
+    using Pp = decltype(P);
+    return run<typename Pp::type, Pp::refine, Pp::uc>(c);
+  });
 }
 
 struct GradCall {
@@ -743,6 +763,7 @@ int run_grad(const GradCall& c) {
 }
 
 int dispatch_grad(const GradCall& c, int precision) {
+  precision &= ~VPM_UNIFORM_CORE;  // the adjoint keeps the general pair core
   if (c.n < 0) return fail(VPM_ERR_ARG, "negative size");
   if (c.n > 0 && (!c.pos || !c.str || !c.rad || !c.ox || !c.oa || !c.os))
     return fail(VPM_ERR_ARG, "null pointer");
@@ -923,43 +944,29 @@ int vpm_device_errors(int* out, int clear) {
 }
 
 size_t vpm_workspace_bytes(int op, int precision, int64_t m, int64_t n) {
-  Plan p;
-  Layout L;
-  int rc;
-  switch (precision) {
-    case VPM_FP64:
-      rc = workspace_for<double, false>(op, m, n, &L, &p);
-      break;
-    case VPM_FP32C:
-      rc = workspace_for<float2, false>(op, m, n, &L, &p);
-      break;
-    case VPM_FP32C_REFINED:
-      rc = workspace_for<float2, true>(op, m, n, &L, &p);
-      break;
-    default:
-      fail(VPM_ERR_ARG, "unknown precision");
-      return 0;
-  }
-  return rc ? 0 : L.total;
+  if (op == VPM_OP_RHS_VJP || op == VPM_OP_RHS_VJP_PSE || op == VPM_OP_KINETIC_ENERGY_GRAD)
+    precision &= ~VPM_UNIFORM_CORE;
+  size_t total = 0;
+  const int rc = with_precision(precision, [&](auto P) {
+    using Pp = decltype(P);
+    Plan p;
+    Layout L;
+    const int r = workspace_for<typename Pp::type, Pp::refine, Pp::uc>(op, m, n, &L, &p);
+    if (!r) total = L.total;
+    return r;
+  });
+  return rc ? 0 : total;
 }
 
 int vpm_plan_info(int op, int precision, int64_t m, int64_t n, int64_t* target_blocks,
                   int* splits, int* threads, int* targets_per_thread) {
+  if (op == VPM_OP_RHS_VJP || op == VPM_OP_RHS_VJP_PSE || op == VPM_OP_KINETIC_ENERGY_GRAD)
+    precision &= ~VPM_UNIFORM_CORE;
   Plan p;
-  int rc;
-  switch (precision) {
-    case VPM_FP64:
-      rc = plan_op<double, false>(op, m, n, &p);
-      break;
-    case VPM_FP32C:
-      rc = plan_op<float2, false>(op, m, n, &p);
-      break;
-    case VPM_FP32C_REFINED:
-      rc = plan_op<float2, true>(op, m, n, &p);
-      break;
-    default:
-      return fail(VPM_ERR_ARG, "unknown precision");
-  }
+  const int rc = with_precision(precision, [&](auto P) {
+    using Pp = decltype(P);
+    return plan_op<typename Pp::type, Pp::refine, Pp::uc>(op, m, n, &p);
+  });
   if (rc) return rc;
   if (target_blocks) *target_blocks = p.tblocks;
   if (splits) *splits = p.splits;
@@ -1063,7 +1070,7 @@ int vpm_les_step_sums(const double* positions, const double* strengths, const do
 }
 
 size_t vpm_record_bytes(int precision) {
-  switch (precision) {
+  switch (precision & ~VPM_UNIFORM_CORE) {
     case VPM_FP64:
       return sizeof(Rec<double>);
     case VPM_FP32C:
@@ -1086,12 +1093,14 @@ int vpm_pack_records(const double* positions, const double* strengths, const dou
   int rc = check_arch();
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const bool uc = (precision & VPM_UNIFORM_CORE) != 0;
+  precision &= ~VPM_UNIFORM_CORE;
   if (precision == VPM_FP64)
     return pack<double>(positions, strengths, radii, viscosities, n,
-                        static_cast<Rec<double>*>(records), st);
+                        static_cast<Rec<double>*>(records), st, uc);
   if (precision == VPM_FP32C || precision == VPM_FP32C_REFINED)
     return pack<float2>(positions, strengths, radii, viscosities, n,
-                        static_cast<Rec<float2>*>(records), st);
+                        static_cast<Rec<float2>*>(records), st, uc);
   return fail(VPM_ERR_ARG, "unknown precision");
 }
 

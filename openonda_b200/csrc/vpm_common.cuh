@@ -20,6 +20,7 @@ constexpr double kRefEps = 1e-8;  // ParticlesPhysicsCuda.py:6
 
 // Device-side error bits (read by vpm_device_errors()).
 constexpr int VPM_DEVERR_WAIT_TIMEOUT = 1;
+constexpr int VPM_DEVERR_NONUNIFORM_CORE = 2;
 
 constexpr unsigned long long VPM_WAIT_LIMIT_NS = 1000000000ull;  // 1 s
 

@@ -67,22 +67,40 @@ __device__ __forceinline__ Src<double> load_src<double>(const Rec<double>& r) {
 // Per-lane target registers shared by all operators.
 template <class V>
 struct Tgt {
-  V x, y, z, hs;  // position, half core
-  V ax, ay, az;   // strength
+  V x, y, z, hs;   // position, half core
+  V ax, ay, az;    // strength
+  V sc, s2c, s4c;  // core, core^2, core^4 (the pair core when all cores are equal)
 };
 
 // `r` points at the lane's records: one for FP64, two (lane 0, lane 1) for FP32.
 __device__ __forceinline__ Tgt<double> make_tgt(const Rec<double>* const* r) {
   const Rec<double>& a = *r[0];
-  return Tgt<double>{a.x, a.y, a.z, 0.5 * a.s, a.ax, a.ay, a.az};
+  const double s2 = a.s * a.s;
+  return Tgt<double>{a.x, a.y, a.z, 0.5 * a.s, a.ax, a.ay, a.az, a.s, s2, s2 * s2};
 }
 __device__ __forceinline__ Tgt<float2> make_tgt(const Rec<float2>* const* r) {
   const Rec<float2>& a = *r[0];
   const Rec<float2>& b = *r[1];
+  const float2 sc = make_float2(a.s.x, b.s.x);
+  const float2 s2 = sc * sc;
   return Tgt<float2>{make_float2(a.x.x, b.x.x),   make_float2(a.y.x, b.y.x),
                      make_float2(a.z.x, b.z.x),   make_float2(0.5f * a.s.x, 0.5f * b.s.x),
                      make_float2(a.ax.x, b.ax.x), make_float2(a.ay.x, b.ay.x),
-                     make_float2(a.az.x, b.az.x)};
+                     make_float2(a.az.x, b.az.x), sc, s2, s2 * s2};
+}
+
+// Pair core s = (sigma_i + sigma_j)/2 and s^2.  UC ("uniform core"): the caller guarantees
+// that every particle has the same core, so s = sigma_i exactly (0.5 s + 0.5 s rounds to s)
+// and s^2 is a per-target constant: two lane-ops fewer per pair, same values.
+template <bool UC, class V>
+__device__ __forceinline__ void pair_core(const Tgt<V>& t, const Src<V>& s, V& sg, V& s2) {
+  if constexpr (UC) {
+    sg = t.sc;
+    s2 = t.s2c;
+  } else {
+    sg = fma(s.s, splat<V>(0.5), t.hs);
+    s2 = sg * sg;
+  }
 }
 
 // Record/lane plumbing shared by the operators on the standard 64-byte record.
@@ -97,14 +115,14 @@ struct PairOpBase {
 };
 
 // ---- self-induced velocity: U += g (r x a_j) ------------------------------------------
-template <class V, bool REFINE>
+template <class V, bool REFINE, bool UC = false>
 struct OpVel : PairOpBase<V> {
   static constexpr int NV = 3;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const V sg = fma(s.s, splat<V>(0.5), t.hs);
-    const V s2 = sg * sg;
+    V sg, s2;
+    pair_core<UC>(t, s, sg, s2);
     const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
     const V y = rsqrt_lane<REFINE>(x);
     const V y2 = y * y;
@@ -162,14 +180,14 @@ struct OpVortAt : PairOpBase<V> {
 };
 
 // ---- stretching (transpose scheme): A += g (a_j - a_i),  B += f (r . (d x a_i)) r -------
-template <class V, bool REFINE>
+template <class V, bool REFINE, bool UC = false>
 struct OpStretch : PairOpBase<V> {
   static constexpr int NV = 6;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const V sg = fma(s.s, splat<V>(0.5), t.hs);
-    const V s2 = sg * sg;
+    V sg, s2;
+    pair_core<UC>(t, s, sg, s2);
     const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
     const V y = rsqrt_lane<REFINE>(x);
     const V y2 = y * y;
@@ -195,14 +213,14 @@ struct OpStretch : PairOpBase<V> {
 #ifndef VPM_Y2_RCP
 #define VPM_Y2_RCP 0
 #endif
-template <class V, bool REFINE>
+template <class V, bool REFINE, bool UC = false>
 struct OpVelStretch : PairOpBase<V> {
   static constexpr int NV = 9;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const V sg = fma(s.s, splat<V>(0.5), t.hs);
-    const V s2 = sg * sg;
+    V sg, s2;
+    pair_core<UC>(t, s, sg, s2);
     const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
     const V y = rsqrt_lane<REFINE>(x);
 #if VPM_Y2_RCP
@@ -245,15 +263,15 @@ struct OpVelStretch : PairOpBase<V> {
 #ifndef VPM_LES_R
 #define VPM_LES_R 2
 #endif
-template <class V, bool REFINE>
+template <class V, bool REFINE, bool UC = false>
 struct OpLesStep : PairOpBase<V> {
   static constexpr int kR = VPM_LES_R;
   static constexpr int NV = 15;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;  // 3
-    const V sg = fma(s.s, splat<V>(0.5), t.hs);                // 1
-    const V s2 = sg * sg;                                      // 1
+    V sg, s2;
+    pair_core<UC>(t, s, sg, s2);                               // 2 (0 with UC)
     const V r2 = fma(rx, rx, fma(ry, ry, rz * rz));            // 3
     const V x = r2 + s2;                                       // 1
     const V y = rsqrt_lane<REFINE>(x);
@@ -276,12 +294,13 @@ struct OpLesStep : PairOpBase<V> {
     acc[7] = fma(h, ry, acc[7]);
     acc[8] = fma(h, rz, acc[8]);
     // vorticity filter sum (source core)
-    const V sj2 = s.s * s.s;                                   // 1
+    const V sj2 = UC ? t.s2c : s.s * s.s;                      // 1 (0 with UC)
     const V yv = rsqrt_lane<REFINE>(r2 + sj2);                 // 1
     const V yv2 = yv * yv;                                     // 4
     const V yv3 = yv2 * yv;
     const V yv7 = (yv3 * yv3) * yv;
-    const V kv = keep_if_gt(r2, kRefEps, (sj2 * sj2) * yv7);   // 2 (+ compare/select)
+    const V sj4 = UC ? t.s4c : sj2 * sj2;                      // 1 (0 with UC)
+    const V kv = keep_if_gt(r2, kRefEps, sj4 * yv7);           // 1 (+ compare/select)
     acc[9] = fma(kv, s.ax, acc[9]);                            // 3
     acc[10] = fma(kv, s.ay, acc[10]);
     acc[11] = fma(kv, s.az, acc[11]);
@@ -294,14 +313,14 @@ struct OpLesStep : PairOpBase<V> {
 };
 
 // ---- PSE diffusion: P += s^7 y^9 (a_j - a_i)  (nu_i applied in finalize) -----------------
-template <class V, bool REFINE>
+template <class V, bool REFINE, bool UC = false>
 struct OpPse : PairOpBase<V> {
   static constexpr int NV = 3;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const V sg = fma(s.s, splat<V>(0.5), t.hs);
-    const V s2 = sg * sg;
+    V sg, s2;
+    pair_core<UC>(t, s, sg, s2);
     const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
     const V y = rsqrt_lane<REFINE>(x);
     const V z = sg * y;  // <= 1
@@ -316,14 +335,14 @@ struct OpPse : PairOpBase<V> {
 };
 
 // ---- enstrophy filter sum (all pairs incl. i == j): V += (x + 2.2 s^2) y^3 a_j ---------
-template <class V, bool REFINE>
+template <class V, bool REFINE, bool UC = false>
 struct OpEns : PairOpBase<V> {
   static constexpr int NV = 3;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t*, int64_t) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const V sg = fma(s.s, splat<V>(0.5), t.hs);
-    const V s2 = sg * sg;
+    V sg, s2;
+    pair_core<UC>(t, s, sg, s2);
     const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
     const V y = rsqrt_lane<REFINE>(x);
     const V y3 = (y * y) * y;
@@ -335,14 +354,14 @@ struct OpEns : PairOpBase<V> {
 };
 
 // ---- kinetic energy (j != i): K += (y + s^2 y^3) a_j + y^3 (r . a_j) r ------------------
-template <class V, bool REFINE>
+template <class V, bool REFINE, bool UC = false>
 struct OpKe : PairOpBase<V> {
   static constexpr int NV = 3;
   __device__ __forceinline__ static void pair(const Tgt<V>& t, V* acc, const Src<V>& s,
                                               const int64_t* i, int64_t j) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
-    const V sg = fma(s.s, splat<V>(0.5), t.hs);
-    const V s2 = sg * sg;
+    V sg, s2;
+    pair_core<UC>(t, s, sg, s2);
     const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
     const V y = rsqrt_lane<REFINE>(x);
     const V y3 = (y * y) * y;

@@ -12,6 +12,11 @@ stream, and returns new CUDA tensors (scalars as 0-d tensors, without a host syn
   windows of 32 sources carried in FP64, FP64 outputs.
 * ``"fp32c_refined"`` -- as ``fp32c`` with one Newton step on the hardware rsqrt.
 
+``uniform_core=True`` (self sums): the caller guarantees that all radii are equal; the pair
+core is then sigma_i and the sweeps skip forming it (same values, 2 FP32 operations fewer per
+pair).  The library checks the claim while packing and reports a false one through
+:func:`device_errors` (bit 1).  ``ParticleSystem`` sets it by itself when its cores are equal.
+
 Scratch space comes from PyTorch's caching allocator and is handed to the C ABI.
 """
 from __future__ import annotations
@@ -66,29 +71,31 @@ def _stream(dev):
     return torch.cuda.current_stream(dev).cuda_stream
 
 
-def workspace_bytes(op: str, precision: str, m: int, n: int) -> int:
+def workspace_bytes(op: str, precision: str, m: int, n: int, uniform_core: bool = False) -> int:
     lib = _lib.load()
-    nbytes = lib.vpm_workspace_bytes(_lib.OPS[op], _lib.precision_code(precision), int(m), int(n))
+    nbytes = lib.vpm_workspace_bytes(_lib.OPS[op], _lib.precision_code(precision, uniform_core),
+                                     int(m), int(n))
     if nbytes == 0 and m > 0 and n > 0:
         msg = lib.vpm_last_error()
         raise _lib.VPMError(_lib.VPM_ERR_CUDA, msg.decode() if msg else "workspace query failed")
     return int(nbytes)
 
 
-def plan_info(op: str, precision: str, m: int, n: int) -> dict:
+def plan_info(op: str, precision: str, m: int, n: int, uniform_core: bool = False) -> dict:
     import ctypes
 
     lib = _lib.load()
     tb, sp, th, r = ctypes.c_int64(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-    _lib.check(lib.vpm_plan_info(_lib.OPS[op], _lib.precision_code(precision), int(m), int(n),
+    _lib.check(lib.vpm_plan_info(_lib.OPS[op], _lib.precision_code(precision, uniform_core),
+                                 int(m), int(n),
                                  ctypes.byref(tb), ctypes.byref(sp), ctypes.byref(th),
                                  ctypes.byref(r)))
     return dict(target_blocks=tb.value, splits=sp.value, threads=th.value,
                 targets_per_thread=r.value)
 
 
-def _workspace(op, precision, m, n, dev):
-    nbytes = workspace_bytes(op, precision, m, n)
+def _workspace(op, precision, m, n, dev, uniform_core=False):
+    nbytes = workspace_bytes(op, precision, m, n, uniform_core)
     return torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev), nbytes
 
 
@@ -101,38 +108,43 @@ def _self_inputs(positions, strengths, radii):
     return positions, strengths, radii, n, dev
 
 
-def selfinduced_velocity(positions, strengths, radii, precision="fp64"):
+def selfinduced_velocity(positions, strengths, radii, precision="fp64", uniform_core=False):
     x, a, s, n, dev = _self_inputs(positions, strengths, radii)
     out = torch.empty((n, 3), dtype=_F64, device=dev)
-    ws, nb = _workspace("selfinduced_velocity", precision, n, n, dev)
+    ws, nb = _workspace("selfinduced_velocity", precision, n, n, dev, uniform_core)
     _lib.check(_lib.load().vpm_selfinduced_velocity(
-        _ptr(x), _ptr(a), _ptr(s), n, _ptr(out), _lib.precision_code(precision), _ptr(ws),
+        _ptr(x), _ptr(a), _ptr(s), n, _ptr(out),
+        _lib.precision_code(precision, uniform_core), _ptr(ws),
         ws.numel(), _stream(dev)))
     return out
 
 
-def strength_gradients(positions, strengths, radii, precision="fp64"):
+def strength_gradients(positions, strengths, radii, precision="fp64", uniform_core=False):
     x, a, s, n, dev = _self_inputs(positions, strengths, radii)
     out = torch.empty((n, 3), dtype=_F64, device=dev)
-    ws, nb = _workspace("strength_gradients", precision, n, n, dev)
+    ws, nb = _workspace("strength_gradients", precision, n, n, dev, uniform_core)
     _lib.check(_lib.load().vpm_strength_gradients(
-        _ptr(x), _ptr(a), _ptr(s), n, _ptr(out), _lib.precision_code(precision), _ptr(ws),
+        _ptr(x), _ptr(a), _ptr(s), n, _ptr(out),
+        _lib.precision_code(precision, uniform_core), _ptr(ws),
         ws.numel(), _stream(dev)))
     return out
 
 
-def velocity_and_strength_gradients(positions, strengths, radii, precision="fp64"):
+def velocity_and_strength_gradients(positions, strengths, radii,
+                                    precision="fp64", uniform_core=False):
     x, a, s, n, dev = _self_inputs(positions, strengths, radii)
     u = torch.empty((n, 3), dtype=_F64, device=dev)
     g = torch.empty((n, 3), dtype=_F64, device=dev)
-    ws, nb = _workspace("velocity_and_strength_gradients", precision, n, n, dev)
+    ws, nb = _workspace("velocity_and_strength_gradients", precision, n, n, dev, uniform_core)
     _lib.check(_lib.load().vpm_velocity_and_strength_gradients(
-        _ptr(x), _ptr(a), _ptr(s), n, _ptr(u), _ptr(g), _lib.precision_code(precision),
+        _ptr(x), _ptr(a), _ptr(s), n, _ptr(u), _ptr(g),
+        _lib.precision_code(precision, uniform_core),
         _ptr(ws), ws.numel(), _stream(dev)))
     return u, g
 
 
-def les_step_sums(positions, strengths, radii, ref_extra_4pi=True, precision="fp64"):
+def les_step_sums(positions, strengths, radii, ref_extra_4pi=True,
+                  precision="fp64", uniform_core=False):
     """Velocity, stretching, particle vorticity and the enstrophy filter sum of one
     dynamic-LES step, from one sweep over the same state.  Returns (u, dalpha_dt, omega,
     enstrophy) with the enstrophy as a 0-d tensor."""
@@ -141,22 +153,25 @@ def les_step_sums(positions, strengths, radii, ref_extra_4pi=True, precision="fp
     g = torch.empty((n, 3), dtype=_F64, device=dev)
     w = torch.empty((n, 3), dtype=_F64, device=dev)
     e = torch.empty((), dtype=_F64, device=dev)
-    ws, nb = _workspace("les_step_sums", precision, n, n, dev)
+    ws, nb = _workspace("les_step_sums", precision, n, n, dev, uniform_core)
     _lib.check(_lib.load().vpm_les_step_sums(
         _ptr(x), _ptr(a), _ptr(s), n, _ptr(u), _ptr(g), _ptr(w), _ptr(e),
-        int(bool(ref_extra_4pi)), _lib.precision_code(precision), _ptr(ws), ws.numel(),
+        int(bool(ref_extra_4pi)),
+        _lib.precision_code(precision, uniform_core), _ptr(ws), ws.numel(),
         _stream(dev)))
     return u, g, w, e
 
 
-def strength_gradients_pse(positions, strengths, radii, viscosities, precision="fp64"):
+def strength_gradients_pse(positions, strengths, radii, viscosities,
+                           precision="fp64", uniform_core=False):
     x, a, s, n, dev = _self_inputs(positions, strengths, radii)
     v = _check_scalar("viscosities", viscosities, n)
     _same_device(x, v)
     out = torch.empty((n, 3), dtype=_F64, device=dev)
-    ws, nb = _workspace("strength_gradients_pse", precision, n, n, dev)
+    ws, nb = _workspace("strength_gradients_pse", precision, n, n, dev, uniform_core)
     _lib.check(_lib.load().vpm_strength_gradients_pse(
-        _ptr(x), _ptr(a), _ptr(s), _ptr(v), n, _ptr(out), _lib.precision_code(precision),
+        _ptr(x), _ptr(a), _ptr(s), _ptr(v), n, _ptr(out),
+        _lib.precision_code(precision, uniform_core),
         _ptr(ws), ws.numel(), _stream(dev)))
     return out
 
@@ -204,13 +219,14 @@ def total_helicity(positions, strengths, radii, ref_extra_4pi=True, precision="f
     return out
 
 
-def total_enstrophy(positions, strengths, radii, ref_extra_4pi=True, precision="fp64"):
+def total_enstrophy(positions, strengths, radii, ref_extra_4pi=True,
+                    precision="fp64", uniform_core=False):
     x, a, s, n, dev = _self_inputs(positions, strengths, radii)
     out = torch.empty((), dtype=_F64, device=dev)
-    ws, nb = _workspace("total_enstrophy", precision, n, n, dev)
+    ws, nb = _workspace("total_enstrophy", precision, n, n, dev, uniform_core)
     _lib.check(_lib.load().vpm_total_enstrophy(
         _ptr(x), _ptr(a), _ptr(s), n, int(bool(ref_extra_4pi)), _ptr(out),
-        _lib.precision_code(precision), _ptr(ws), ws.numel(), _stream(dev)))
+        _lib.precision_code(precision, uniform_core), _ptr(ws), ws.numel(), _stream(dev)))
     return out
 
 

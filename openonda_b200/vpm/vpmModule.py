@@ -148,6 +148,8 @@ class ParticleSystem:
         self._rate_token = None
         self._les_w = None  # LES vorticity / enstrophy from the same sweep (same token)
         self._les_ens = None
+        self._uc = False  # all cores equal: sums use the uniform-core form
+        self._nu_uniform = self._nut_uniform = False
         self._graph = None  # captured steady-state step (advance)
         self._graph_x_next = None
         self._graph_key_val = None
@@ -434,7 +436,20 @@ class ParticleSystem:
             self._gid = np.concatenate([self._gid, np.asarray(gid, np.int64).reshape(-1)])
         self._n = int(self._x.shape[0])
         self._hist = None if self._hist is None else self._resize_hist()
+        self._update_uniformity()
         self._touch()
+
+    def _update_uniformity(self):
+        """Whether all cores are equal, in which case the pair sums take the uniform-core form
+        (the pair core is sigma_i; 2 FP32 operations fewer per pair, same values).  One
+        device reduction per change of the particle set."""
+        if self._n == 0:
+            self._uc = self._nu_uniform = self._nut_uniform = False
+            return
+        same = lambda t: bool((t == t[0]).all())
+        self._uc = same(self._s)
+        self._nu_uniform = same(self._nu)
+        self._nut_uniform = same(self._nut)
 
     def _resize_hist(self):
         n = self._n
@@ -456,6 +471,7 @@ class ParticleSystem:
         if self._hist is not None:
             self._hist = [h[m].contiguous() for h in self._hist]
         self._n = int(self._x.shape[0])
+        self._update_uniformity()
         self._touch()
 
     def remove_particles(self, particle_indices: list):
@@ -553,7 +569,8 @@ class ParticleSystem:
         self.time_step_size = time_step_size
 
     def _vel(self, x):
-        return kernels.selfinduced_velocity(x, self._a, self._s, precision=self.precision)
+        return kernels.selfinduced_velocity(x, self._a, self._s, precision=self.precision,
+                                            uniform_core=self._uc)
 
     def _axpy(self, x, k, c):
         out = torch.empty_like(x)
@@ -633,7 +650,7 @@ class ParticleSystem:
         ts = [self._x, self._a, self._u, self._s, self._nu, self._nut, self._les]
         ts += list(self._hist or [])
         return (self._n, float(self.time_step_size), self.time_integration_method.strip(),
-                self.flow_model, self.viscous_scheme, self.precision,
+                self.flow_model, self.viscous_scheme, self.precision, self._uc,
                 bool(self.relax_strength_solution),
                 tuple(0 if t is None else t.data_ptr() for t in ts))
 
@@ -695,11 +712,12 @@ class ParticleSystem:
         if self.flow_model == "LES":
             # one sweep also yields the two LES filter sums update_strengths needs next
             self._u, self._rate, self._les_w, self._les_ens = kernels.les_step_sums(
-                self._x, self._a, self._s, ref_extra_4pi=True, precision=self.precision)
+                self._x, self._a, self._s, ref_extra_4pi=True, precision=self.precision,
+                uniform_core=self._uc)
             self._rate_token = self._token
         elif self.flow_model == "DNS":
             self._u, self._rate = kernels.velocity_and_strength_gradients(
-                self._x, self._a, self._s, precision=self.precision)
+                self._x, self._a, self._s, precision=self.precision, uniform_core=self._uc)
             self._rate_token = self._token
         else:
             self._u = self._vel(self._x)
@@ -708,7 +726,8 @@ class ParticleSystem:
     def _stretching_rate(self):
         if self._rate is not None and self._rate_token == self._token:
             return self._rate
-        return kernels.strength_gradients(self._x, self._a, self._s, precision=self.precision)
+        return kernels.strength_gradients(self._x, self._a, self._s, precision=self.precision,
+                                          uniform_core=self._uc)
 
     def _bdf(self, rate):
         if self._hist is None:
@@ -736,7 +755,7 @@ class ParticleSystem:
             else:
                 w = self._vorticity()
                 ens = kernels.total_enstrophy(self._x, self._a, self._s, ref_extra_4pi=True,
-                                              precision=self.precision)
+                                              precision=self.precision, uniform_core=self._uc)
             self._les_w = self._les_ens = None
             self._les_update(w, ens)
         rate_s = None
@@ -750,13 +769,17 @@ class ParticleSystem:
         if self.viscous_scheme == "PSE":
             nu_eff = self._nu + self._nut
             rate_p = kernels.strength_gradients_pse(self._x, self._a, self._s, nu_eff,
-                                                    precision=self.precision)
+                                                    precision=self.precision,
+                                                    uniform_core=self._uc)
             self._bdf(rate_p)
             self._touch()
         elif self.viscous_scheme == "CoreSpreading":
             _check(_lib.load().vpm_core_spreading(
                 self._s.data_ptr(), self._nu.data_ptr(), self._nut.data_ptr(), self._n,
                 CORE_SPREADING_C, float(self.time_step_size), _stream(dev)))
+            # equal cores stay equal (bitwise) when every particle has the same nu + nu_t
+            self._uc = (self._uc and self._nu_uniform and self._nut_uniform
+                        and self.flow_model != "LES")
             self._touch()
         if self.relax_strength_solution:
             w = self._vorticity()

@@ -17,6 +17,7 @@ config5  dynamic-LES ring N=2^20, FP32c, PSE, RK4 dt=0.002: time per step, Gpair
          FP64 at the last step.
 stepkernels  GB/s of the element-wise step kernels (RK stage, RK4 combine, BDF) at N=2^22.
 sweeps       time of each FP32c sweep of an LES step (fused LES sums vs the sweeps they replace).
+peaks        FP32 FFMA / FFMA2 / mixed / MUFU rsqrt throughput microbenchmarks.
 
 All inputs are the seeded synthetic fields of :mod:`openonda_b200.configs`.
 """
@@ -241,6 +242,7 @@ def config5(args):
     steps = args.steps or 100
     ps = _system(f, "fp32c", flow_model="LES", viscous_scheme="PSE",
                  time_integration_method="RK4", time_step_size=0.002)
+    assert ps._uc  # one core for the whole ring: the uniform-core sweeps
     t_total = 0.0
     for k in range(steps):
         with _Timer() as t:
@@ -248,10 +250,15 @@ def config5(args):
         t_total += t.ms
     eu, eg = _errors_vs_fp64(ps)
     n = f.n
-    sweeps = 7.0  # fused vel+stretch, vorticity, enstrophy, PSE, 3 RK stages
+    # 7 N^2 pair sums per step as the reference counts them (velocity + stretching counted
+    # once), run here as 5 sweeps: LES step sums (velocity, stretching, vorticity,
+    # enstrophy), PSE and 3 RK-stage velocities.  Gpairs/s counts the 7 sums.
+    sums = 7.0
     _emit({"config": "config5", "workload": f.description, "n": n, "steps": steps,
-           "precision": "fp32c", "ms_per_step": round(t_total / steps, 1),
-           "gpairs_per_s": round(sweeps * n * n / (t_total / steps / 1e3) / 1e9, 1),
+           "precision": "fp32c", "uniform_core": ps._uc,
+           "ms_per_step": round(t_total / steps, 1),
+           "pair_sums_per_step": int(sums), "sweeps_per_step": 5,
+           "gpairs_per_s": round(sums * n * n / (t_total / steps / 1e3) / 1e9, 1),
            "rel_err_velocity_last_step": eu, "rel_err_stretching_last_step": eg,
            "cnu": ps.Cnu})
 
@@ -268,24 +275,58 @@ def sweeps(args):
     x, a, s, nu = r(f.positions), r(f.strengths), r(f.radii), r(f.viscosities)
     p = "fp32c"
     cases = {
-        "les_step_sums": lambda: kernels.les_step_sums(x, a, s, precision=p),
+        "les_step_sums": lambda uc: kernels.les_step_sums(x, a, s, precision=p,
+                                                          uniform_core=uc),
         "velocity_and_strength_gradients":
-            lambda: kernels.velocity_and_strength_gradients(x, a, s, precision=p),
-        "vorticity_field_at": lambda: kernels.vorticity_field_at(x, x, a, s, precision=p),
-        "total_enstrophy": lambda: kernels.total_enstrophy(x, a, s, precision=p),
+            lambda uc: kernels.velocity_and_strength_gradients(x, a, s, precision=p,
+                                                               uniform_core=uc),
+        "vorticity_field_at": lambda uc: kernels.vorticity_field_at(x, x, a, s, precision=p),
+        "total_enstrophy": lambda uc: kernels.total_enstrophy(x, a, s, precision=p,
+                                                              uniform_core=uc),
         "strength_gradients_pse":
-            lambda: kernels.strength_gradients_pse(x, a, s, nu, precision=p),
-        "selfinduced_velocity": lambda: kernels.selfinduced_velocity(x, a, s, precision=p),
+            lambda uc: kernels.strength_gradients_pse(x, a, s, nu, precision=p,
+                                                      uniform_core=uc),
+        "selfinduced_velocity": lambda uc: kernels.selfinduced_velocity(x, a, s, precision=p,
+                                                                        uniform_core=uc),
     }
     reps = args.steps or 3
     for name, fn in cases.items():
-        fn()
-        with _Timer() as t:
-            for _ in range(reps):
-                fn()
-        ms = t.ms / reps
-        _emit({"sweep": name, "n": n, "precision": p, "ms": round(ms, 2),
-               "gpairs_per_s": round(float(n) * n / (ms / 1e3) / 1e9, 1)})
+        for uc in (False, True):
+            if uc and name == "vorticity_field_at":
+                continue  # probe sums have no uniform-core form
+            fn(uc)
+            with _Timer() as t:
+                for _ in range(reps):
+                    fn(uc)
+            ms = t.ms / reps
+            _emit({"sweep": name, "uniform_core": uc, "n": n, "precision": p,
+                   "ms": round(ms, 2),
+                   "gpairs_per_s": round(float(n) * n / (ms / 1e3) / 1e9, 1)})
+
+
+def peaks(args):
+    """Throughput of the FP32 pipes by microbenchmark (vpm_launch_fma_peak), at three
+    occupancies: scalar FFMA, packed FFMA2, a 1:1 mix of the two, and MUFU rsqrt; in lane
+    operations per clock per SM at the nominal 1965 MHz."""
+    dev = torch.device("cuda")
+    props = torch.cuda.get_device_properties(dev)
+    for kind, name, lanes in ((0, "ffma", 16), (3, "ffma2", 32), (4, "ffma2+ffma", 32),
+                              (2, "mufu_rsqrt", 16)):
+        for per_sm, threads in ((8, 256), (4, 128), (2, 128)):
+            blocks = props.multi_processor_count * per_sm
+            sink = torch.empty(blocks * threads, dtype=torch.float32, device=dev)
+            iters = 1 << 13
+            kernels.launch_fma_peak(kind, blocks, threads, 64, sink)
+            best = float("inf")
+            for _ in range(5):
+                with _Timer() as t:
+                    kernels.launch_fma_peak(kind, blocks, threads, iters, sink)
+                best = min(best, t.ms / 1e3)
+            ops = blocks * threads * iters * lanes
+            _emit({"pipe": name, "warps_per_sm": per_sm * threads // 32,
+                   "t_lane_ops_per_s": round(ops / best / 1e12, 2),
+                   "lane_ops_per_clk_per_sm": round(ops / best / props.multi_processor_count
+                                                    / 1.965e9, 1)})
 
 
 def stepkernels(args):
@@ -326,7 +367,7 @@ def stepkernels(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("workload", choices=["config1", "config2", "config3", "config4", "config5",
-                                         "stepkernels", "sweeps"])
+                                         "stepkernels", "sweeps", "peaks"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--fd", type=int, default=None)
     ap.add_argument("--n", type=int, default=None)

@@ -329,3 +329,42 @@ def test_les_step_sums_empty_and_errors():
     lib = _lib.load()
     assert lib.vpm_les_step_sums(None, None, None, 4, None, None, None, None, 1, 0, None, 0,
                                  None) == _lib.VPM_ERR_ARG
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_uniform_core_form_matches_general_form(precision):
+    """VPM_UNIFORM_CORE: with all cores equal the pair core is sigma_i, so the specialised
+    sweeps must give the general sweeps' values (same pair terms; only the launch plan, and
+    with it the FP64 summation order, may differ)."""
+    import torch
+
+    from openonda_b200 import configs, kernels
+
+    f = configs.vortex_ring(32, 64, 1.0, 1.0, 0.1, nu=1e-3)  # N = 2048, one core
+    assert np.all(f.radii == f.radii[0])
+    x, a, s, nu = (torch.from_numpy(np.ascontiguousarray(z)).cuda()
+                   for z in (f.positions, f.strengths, f.radii, f.viscosities))
+    kernels.device_errors()
+    tol = 1e-14 if precision == "fp64" else 1e-7
+    pairs = [
+        (kernels.selfinduced_velocity, (x, a, s)),
+        (kernels.strength_gradients, (x, a, s)),
+        (kernels.velocity_and_strength_gradients, (x, a, s)),
+        (kernels.strength_gradients_pse, (x, a, s, nu)),
+        (kernels.les_step_sums, (x, a, s)),
+        (kernels.total_enstrophy, (x, a, s)),
+    ]
+    for fn, args in pairs:
+        ref = fn(*args, precision=precision)
+        got = fn(*args, precision=precision, uniform_core=True)
+        ref = ref if isinstance(ref, tuple) else (ref,)
+        got = got if isinstance(got, tuple) else (got,)
+        for r, g in zip(ref, got):
+            assert normwise(g.cpu().numpy(), r.cpu().numpy()) <= tol, fn.__name__
+    assert kernels.device_errors() == 0
+    # a false claim is flagged (bit 1), not silently accepted
+    s2 = s.clone()
+    s2[5] *= 1.5
+    kernels.selfinduced_velocity(x, a, s2, precision=precision, uniform_core=True)
+    assert kernels.device_errors() & 2
+    assert kernels.device_errors() == 0
