@@ -92,12 +92,17 @@ __device__ __forceinline__ double rsqrt_lane(double x) {
 
 // ---- per-lane selections --------------------------------------------------------------------
 // v where a > thr, else 0
-__device__ __forceinline__ double keep_if_gt(double a, double thr, double v) {
-  return a > thr ? v : 0.0;
+// acc + v * w where a > thr, acc unchanged elsewhere: a skipped pair adds nothing even when
+// its terms are not finite, as with the reference's branch (ParticlesPhysicsCuda.py:80, 332).
+__device__ __forceinline__ double fma_if_gt(double a, double thr, double v, double w,
+                                            double acc) {
+  return a > thr ? fma(v, w, acc) : acc;
 }
-__device__ __forceinline__ float2 keep_if_gt(float2 a, double thr, float2 v) {
+__device__ __forceinline__ float2 fma_if_gt(float2 a, double thr, float2 v, float2 w,
+                                            float2 acc) {
   const float t = float(thr);
-  return make_float2(a.x > t ? v.x : 0.f, a.y > t ? v.y : 0.f);
+  const float2 r = fma(v, w, acc);
+  return make_float2(a.x > t ? r.x : acc.x, a.y > t ? r.y : acc.y);
 }
 // v except in the lanes whose target index equals j
 __device__ __forceinline__ double zero_if_self(double v, const int64_t* i, int64_t j) {

@@ -149,13 +149,13 @@ struct OpVelAt : PairOpBase<V> {
     const V y = rsqrt_lane<REFINE>(r2 + s2);
     const V y2 = y * y;
     const V y5 = (y2 * y2) * y;
-    const V g = keep_if_gt(r2, kRefEps, fma(splat<V>(2.5), s2, r2) * y5);
+    const V g = fma(splat<V>(2.5), s2, r2) * y5;
     const V cx = fma(ry, s.az, -(rz * s.ay));
     const V cy = fma(rz, s.ax, -(rx * s.az));
     const V cz = fma(rx, s.ay, -(ry * s.ax));
-    acc[0] = fma(g, cx, acc[0]);
-    acc[1] = fma(g, cy, acc[1]);
-    acc[2] = fma(g, cz, acc[2]);
+    acc[0] = fma_if_gt(r2, kRefEps, g, cx, acc[0]);
+    acc[1] = fma_if_gt(r2, kRefEps, g, cy, acc[1]);
+    acc[2] = fma_if_gt(r2, kRefEps, g, cz, acc[2]);
   }
 };
 
@@ -172,10 +172,10 @@ struct OpVortAt : PairOpBase<V> {
     const V y2 = y * y;
     const V y3 = y2 * y;
     const V y7 = (y3 * y3) * y;
-    const V k = keep_if_gt(r2, kRefEps, (s2 * s2) * y7);
-    acc[0] = fma(k, s.ax, acc[0]);
-    acc[1] = fma(k, s.ay, acc[1]);
-    acc[2] = fma(k, s.az, acc[2]);
+    const V k = (s2 * s2) * y7;
+    acc[0] = fma_if_gt(r2, kRefEps, k, s.ax, acc[0]);
+    acc[1] = fma_if_gt(r2, kRefEps, k, s.ay, acc[1]);
+    acc[2] = fma_if_gt(r2, kRefEps, k, s.az, acc[2]);
   }
 };
 
@@ -255,10 +255,10 @@ struct OpVelStretch : PairOpBase<V> {
 // (:644, pair core, all pairs).  One sweep gives all 15 sums:
 //   U, A, B as OpVelStretch;  W += s_j^4 y_j^7 a_j  (y_j = (r^2 + s_j^2)^-1/2);
 //   E += (x + 2.2 s^2) y^3 a_j.
-// Per pair 58 FP32 lane-ops and 2 MUFU (counts beside the statements): 39 for velocity and
+// Per pair 56 FP32 lane-ops and 2 MUFU (counts beside the statements): 39 for velocity and
 // stretching (one more than OpVelStretch, since r^2 is formed on its own for the vorticity),
-// 13 for the vorticity (incl. the r^2 test), 6 for the enstrophy; three separate sweeps cost
-// 38 + ~20 + ~15.  15 sums per target do not fit four targets per thread in registers, so
+// 11 for the vorticity, 6 for the enstrophy, plus the vorticity's r^2 test (compare and
+// selects, ALU pipe); three separate sweeps cost 38 + ~20 + ~15.  Uniform cores: 52.  15 sums per target do not fit four targets per thread in registers, so
 // this operator runs two (one packed lane).
 #ifndef VPM_LES_R
 #define VPM_LES_R 2
@@ -300,10 +300,10 @@ struct OpLesStep : PairOpBase<V> {
     const V yv3 = yv2 * yv;
     const V yv7 = (yv3 * yv3) * yv;
     const V sj4 = UC ? t.s4c : sj2 * sj2;                      // 1 (0 with UC)
-    const V kv = keep_if_gt(r2, kRefEps, sj4 * yv7);           // 1 (+ compare/select)
-    acc[9] = fma(kv, s.ax, acc[9]);                            // 3
-    acc[10] = fma(kv, s.ay, acc[10]);
-    acc[11] = fma(kv, s.az, acc[11]);
+    const V kv = sj4 * yv7;                                    // 1
+    acc[9] = fma_if_gt(r2, kRefEps, kv, s.ax, acc[9]);         // 3 (+ compare, selects)
+    acc[10] = fma_if_gt(r2, kRefEps, kv, s.ay, acc[10]);
+    acc[11] = fma_if_gt(r2, kRefEps, kv, s.az, acc[11]);
     // enstrophy filter sum (pair core)
     const V ke = fma(splat<V>(2.2), s2, x) * (y2 * y);         // 3
     acc[12] = fma(ke, s.ax, acc[12]);                          // 3

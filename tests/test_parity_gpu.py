@@ -368,3 +368,28 @@ def test_uniform_core_form_matches_general_form(precision):
     kernels.selfinduced_velocity(x, a, s2, precision=precision, uniform_core=True)
     assert kernels.device_errors() & 2
     assert kernels.device_errors() == 0
+
+
+def test_non_finite_input_propagates_like_reference(pp):
+    """A NaN position reaches every target of the self sums (as in the reference, which has
+    no guard), while the probe sums skip the pair (their r^2 > 1e-8 test is false for NaN,
+    ParticlesPhysicsCuda.py:77) -- same NaN pattern as the oracle, no fault."""
+    from openonda_b200 import configs
+
+    f = configs.random_cloud(300, seed=8)
+    x = f.positions.copy()
+    x[17, 1] = np.nan
+    t = f.positions[:40] * 0.9
+    o = oracle.gpu
+    for name in ("get_selfinduced_velocity", "get_strength_gradients"):
+        got = getattr(pp, name)(x, f.strengths, f.radii)
+        ref = getattr(o, name)(x, f.strengths, f.radii)
+        assert np.array_equal(np.isnan(got), np.isnan(ref)), name
+        assert np.isnan(got).all(), name
+    got = pp.get_induced_velocity_at(t, x, f.strengths, f.radii)
+    ref = o.get_induced_velocity_at(t, x, f.strengths, f.radii)
+    assert np.array_equal(np.isnan(got), np.isnan(ref))
+    assert normwise(got, ref) <= FP64_TOL
+    from openonda_b200 import kernels
+
+    assert kernels.device_errors() == 0
