@@ -660,7 +660,8 @@ class ParticleSystem:
         for op in ("selfinduced_velocity", "velocity_and_strength_gradients", "les_step_sums",
                    "strength_gradients", "strength_gradients_pse", "vorticity_field_at",
                    "total_enstrophy"):
-            kernels.plan_info(op, self.precision, self._n, self._n)
+            kernels.plan_info(op, self.precision, self._n, self._n,
+                              uniform_core=self._uc and op != "vorticity_field_at")
 
     def _capture_step(self):
         dev = self._dev()

@@ -240,6 +240,14 @@ GRAPH_CASES = {
 }
 
 
+GRAPH_CASES["ring_dns_pse_rk4_uniform_core"] = dict(
+    flow_model="DNS", viscous_scheme="PSE", time_integration_method="RK4",
+    time_step_size=0.005, field="ring")
+GRAPH_CASES["ring_dns_cs_rk2_uniform_core"] = dict(
+    flow_model="DNS", viscous_scheme="CoreSpreading", time_integration_method="RK2",
+    time_step_size=0.005, field="ring")
+
+
 @pytest.mark.parametrize("name", sorted(GRAPH_CASES))
 def test_advance_with_cuda_graph_equals_eager_loop(tmp_path, name):
     """advance() replays one captured step from time step 3 on; it must reproduce the
@@ -247,8 +255,8 @@ def test_advance_with_cuda_graph_equals_eager_loop(tmp_path, name):
     including the steps where a backup is due and after a change that forces a recapture."""
     import torch
 
-    f = _field("cloud")
-    cfg = GRAPH_CASES[name]
+    cfg = dict(GRAPH_CASES[name])
+    f = _field(cfg.pop("field", "cloud"))
     from openonda_b200.vpm.vpmModule import ParticleSystem
 
     def make(sub):
@@ -261,8 +269,11 @@ def test_advance_with_cuda_graph_equals_eager_loop(tmp_path, name):
     os.makedirs(tmp_path / "e", exist_ok=True)
     os.makedirs(tmp_path / "g", exist_ok=True)
     eager, graph = make("e"), make("g")
+    # ring fields have one core (uniform-core sweeps, kept through core spreading)
+    assert graph._uc == bool(np.all(f.radii == f.radii[0]))
     _run(eager, 9)
     graph.advance(9)
+    assert graph._uc == eager._uc
     assert graph._graph is not None  # steps 3..8 replayed
     eager.update_dt(0.004)  # settings change: the next graph step captures again
     graph.update_dt(0.004)
@@ -275,4 +286,7 @@ def test_advance_with_cuda_graph_equals_eager_loop(tmp_path, name):
     assert eager.time_step == graph.time_step == 12
     assert eager.flow_time == graph.flow_time
     assert eager.Cnu == graph.Cnu
+    from openonda_b200 import kernels
+
+    assert kernels.device_errors() == 0  # no false uniform-core claim
     torch.cuda.synchronize()
