@@ -85,25 +85,9 @@ __device__ __forceinline__ float2 rsqrt_lane(float2 x) {
     return make_float2(rsqrt_approx(x.x), rsqrt_approx(x.y));
   }
 }
-#ifndef VPM_F64_RSQRT_NEWTON
-#define VPM_F64_RSQRT_NEWTON 0
-#endif
 template <bool REFINE>
 __device__ __forceinline__ double rsqrt_lane(double x) {
-#if VPM_F64_RSQRT_NEWTON
-  // FP32 hardware estimate (relative error ~2^-22), then two Newton-Raphson steps
-  // y <- y + (y/2)(1 - x y^2) in FP64; the relative error squares at each step.  Outside the
-  // FP32 normal range the estimate is not usable and CUDA's rsqrt() is taken.
-  if (x > 1.2e-38 && x < 3.0e38) {
-    double y = double(rsqrt_approx(float(x)));
-#pragma unroll
-    for (int k = 0; k < 2; ++k) y = fma(0.5 * y, fma(-(x * y), y, 1.0), y);
-    return y;
-  }
   return rsqrt(x);
-#else
-  return rsqrt(x);
-#endif
 }
 
 // ---- per-lane selections --------------------------------------------------------------------

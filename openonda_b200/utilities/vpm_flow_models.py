@@ -4,8 +4,9 @@ Same functions, arguments and return values as OpenONDA/utilities/vpm_flow_model
 (``lamb_oseen_vpm`` :14-83, ``vortex_ring_vpm`` :87-163): numpy inputs give numpy outputs,
 CUDA tensors give CUDA tensors.  The per-particle work and the circulation rescaling of the
 ring run in the library kernels (``vpm_ic_lamb_oseen``, ``vpm_ic_vortex_ring``).
-``isotropic_turbulence_vpm`` (an FFT synthesis seeded through numpy's global generator) is
-not provided here.
+``isotropic_turbulence_vpm`` (:167-271) runs its FFT synthesis on the GPU (cuFFT through
+torch.fft) with the same random phases (numpy's MT19937 stream for seed 0, drawn on the
+host from a private generator instead of re-seeding the global one).
 """
 from __future__ import annotations
 
@@ -87,3 +88,49 @@ def vortex_ring_vpm(particle_positions, volumes, particle_radius: float,
     if n and not bool(torch.isfinite(out[1]).all()):
         raise ZeroDivisionError("vortex_ring_vpm: the particles carry no circulation")
     return _finish(tensor_in, out)
+
+
+def isotropic_turbulence_vpm(box_size: float, particle_distance: float, particle_radius: float,
+                             device=None):
+    """Particles on a cubic lattice carrying a synthetic isotropic velocity field with a
+    k^-5/3 spectrum and a Gaussian cut-off at k_max/3 (vpm_flow_models.py:167-271).
+    Returns (positions, velocities, strengths, radii): numpy arrays, or CUDA tensors when
+    ``device`` names a CUDA device.
+
+    Kept as in the reference: the three velocity components share one set of random phases
+    before the divergence-free projection, and each vorticity component keeps only the first
+    of its two central differences (the reference's second term is a separate statement
+    whose value is discarded, :250-262), so omega = (du_z/dy, du_x/dz, du_y/dx)."""
+    dev = cuda_device(device)
+    axis = np.arange(-box_size / 2, box_size / 2, step=particle_distance)
+    n = len(axis)
+    L = box_size
+    k_diss = (np.pi * n / L) / 3
+    ax = torch.from_numpy(axis).to(dev)
+    xx, yy, zz = torch.meshgrid(ax, ax, ax, indexing="ij")
+    positions = torch.stack([xx.reshape(-1), yy.reshape(-1), zz.reshape(-1)], dim=1)
+    k = torch.from_numpy(np.fft.fftfreq(n, L / n) * 2 * np.pi).to(dev)
+    KX, KY, KZ = torch.meshgrid(k, k, k, indexing="ij")
+    K = torch.sqrt(KX * KX + KY * KY + KZ * KZ)
+    E = K ** (-5 / 3) * torch.exp(-((K / k_diss) ** 2))
+    E[K == 0] = 0
+    phases = torch.exp((2j * np.pi) * torch.from_numpy(np.random.RandomState(0).rand(n, n, n))
+                       .to(dev))
+    amp = torch.sqrt(E)
+    ux, uy, uz = amp * phases, amp * phases, amp * phases
+    Kd = K + 1e-10
+    dot = (KX * ux + KY * uy + KZ * uz) / Kd
+    ux = ux - dot * KX / Kd
+    uy = uy - dot * KY / Kd
+    uz = uz - dot * KZ / Kd
+    u = [torch.fft.ifftn(c).real for c in (ux, uy, uz)]
+    velocities = torch.stack([c.reshape(-1) for c in u], dim=1)
+    h2 = 2 * particle_distance
+    w0 = (torch.roll(u[2], -1, dims=1) - torch.roll(u[2], 1, dims=1)) / h2
+    w1 = (torch.roll(u[0], -1, dims=2) - torch.roll(u[0], 1, dims=2)) / h2
+    w2 = (torch.roll(u[1], -1, dims=0) - torch.roll(u[1], 1, dims=0)) / h2
+    strengths = (torch.stack([w0.reshape(-1), w1.reshape(-1), w2.reshape(-1)], dim=1)
+                 * (4 / 3) * particle_distance ** 3)
+    radii = torch.full((n ** 3,), float(particle_radius), dtype=torch.float64, device=dev)
+    out = (positions.contiguous(), velocities.contiguous(), strengths.contiguous(), radii)
+    return out if device is not None else tuple(t.cpu().numpy() for t in out)

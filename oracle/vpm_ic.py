@@ -9,6 +9,7 @@ Restates, in numpy with the reference's operation order:
 * ``get_2D_rectangular_point_distribuition`` -- vpm_solver_helper.py:71-117
 * ``get_hexagonal_point_distribution``       -- vpm_solver_helper.py:120-161
 * ``get_cylindrical_point_distribuition``    -- vpm_solver_helper.py:164-253
+* ``isotropic_turbulence_vpm`` -- OpenONDA/utilities/vpm_flow_models.py:167-271
 
 Pinned by tests/test_ic_oracle.py against tests/golden/ic.npz, which holds the reference
 functions' own outputs (tests/golden/make_golden.py, job ``ic``).  The reference compiles the
@@ -146,3 +147,33 @@ def get_cylindrical_point_distribuition(particle_distance, radius=1.0, height=2.
     axis_pts = np.stack([ax[0] + c[0], ax[1] + c[1], ax[2] + c[2]], axis=1)
     axis_vol = np.full(len(z), np.pi * (radius ** 2) * dz / len(z))
     return np.concatenate([body, axis_pts]), np.concatenate([vol, axis_vol])
+
+
+def isotropic_turbulence_vpm(box_size, particle_distance, particle_radius):
+    """vpm_flow_models.py:167-271 (numpy FFTs; phases from numpy's MT19937 stream for seed 0;
+    each vorticity component keeps only the first central difference, as the reference's
+    second term is a discarded statement)."""
+    x = np.arange(-box_size / 2, box_size / 2, step=particle_distance)
+    n, L = len(x), box_size
+    xx, yy, zz = np.meshgrid(x, x, x, indexing="ij")
+    pts = np.vstack([xx.ravel(), yy.ravel(), zz.ravel()]).T
+    k_diss = (np.pi * n / L) / 3
+    k = np.fft.fftfreq(n, L / n) * 2 * np.pi
+    KX, KY, KZ = np.meshgrid(k, k, k, indexing="ij")
+    K = np.sqrt(KX * KX + KY * KY + KZ * KZ)
+    with np.errstate(divide="ignore"):
+        E = K ** (-5 / 3) * np.exp(-((K / k_diss) ** 2))
+    E[K == 0] = 0
+    ph = np.exp(2j * np.pi * np.random.RandomState(0).rand(n, n, n))
+    ux, uy, uz = np.sqrt(E) * ph, np.sqrt(E) * ph, np.sqrt(E) * ph
+    Kd = K + 1e-10
+    dot = (KX * ux + KY * uy + KZ * uz) / Kd
+    ux, uy, uz = ux - dot * KX / Kd, uy - dot * KY / Kd, uz - dot * KZ / Kd
+    u = [np.real(np.fft.ifftn(c)) for c in (ux, uy, uz)]
+    vel = np.stack([c.reshape(-1) for c in u], axis=1)
+    h2 = 2 * particle_distance
+    w = np.stack([((np.roll(u[2], -1, axis=1) - np.roll(u[2], 1, axis=1)) / h2).reshape(-1),
+                  ((np.roll(u[0], -1, axis=2) - np.roll(u[0], 1, axis=2)) / h2).reshape(-1),
+                  ((np.roll(u[1], -1, axis=0) - np.roll(u[1], 1, axis=0)) / h2).reshape(-1)],
+                 axis=1)
+    return pts, vel, w * (4 / 3) * particle_distance ** 3, np.full(len(pts), particle_radius)

@@ -20,7 +20,7 @@ It executes the reference's own code and writes ``tests/golden/*.npz``:
 * ``steps_gpu.npz``    -- ``vpmModule.ParticleSystem`` with the Numba-CUDA module under the
   simulator (GPU semantics), small N.
 * ``ic.npz``           -- ``OpenONDA/utilities/vpm_flow_models.py`` (vortex_ring_vpm,
-  lamb_oseen_vpm) and ``vpm_solver_helper.py`` (rectangular, 2-D rectangular, hexagonal and
+  lamb_oseen_vpm, isotropic_turbulence_vpm) and ``vpm_solver_helper.py`` (rectangular, 2-D rectangular, hexagonal and
   cylindrical lattices) on the seeded cases of ``ic_cases()``.
 * ``step_ring8192.npz`` -- one DNS+PSE+RK4 step of the 8192-particle ring through the
   reference ``ParticleSystem`` sequencing with the GPU-semantics oracle kernels injected as
@@ -373,6 +373,8 @@ def ic_cases():
                       axis="y"),
         "cyl_z": dict(d=0.09, radius=0.5, height=0.8, center=np.array([-1.0, 0.0, 2.0]),
                       axis="z"),
+        "turb8": dict(box=1.0, d=0.125, radius=0.2),
+        "turb16": dict(box=2.0, d=0.125, radius=0.15),
     }
 
 
@@ -394,6 +396,12 @@ def make_ic(ref):
             fn = (sh.get_rectangular_point_distribuition if name != "rect2"
                   else sh.get_2D_rectangular_point_distribuition)
             out[f"{name}/points"], out[f"{name}/volumes"] = fn(c["box"], c["spacing"])
+        elif name.startswith("turb"):
+            state = np.random.get_state()  # the reference re-seeds numpy's global generator
+            res = fm.isotropic_turbulence_vpm(c["box"], c["d"], c["radius"])
+            np.random.set_state(state)
+            for k, v in zip(("positions", "velocities", "strengths", "radii"), res):
+                out[f"{name}/{k}"] = v
         elif name == "hex":
             out[f"{name}/points"], out[f"{name}/volumes"] = sh.get_hexagonal_point_distribution(
                 c["box"], c["spacing"])

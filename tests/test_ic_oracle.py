@@ -13,6 +13,8 @@ TOL = 1e-14
 
 
 def _oracle(name, c):
+    if name.startswith("turb"):
+        return vpm_ic.isotropic_turbulence_vpm(c["box"], c["d"], c["radius"])
     if name.startswith("ring"):
         return vpm_ic.vortex_ring_vpm(c["positions"], c["volumes"], *c["args"])
     if name == "lamb":
@@ -33,6 +35,8 @@ def test_ic_oracle_vs_reference(name):
     out = _oracle(name, CASES[name])
     if name.startswith("ring") or name == "lamb":
         keys = ("velocities", "strengths", "radii", "viscosities")
+    elif name.startswith("turb"):
+        keys = ("positions", "velocities", "strengths", "radii")
     else:
         keys = ("points", "volumes")
     for k, v in zip(keys, out):
