@@ -17,7 +17,8 @@ FP32-compensated path with ``set_precision("fp32c")`` or per call with
 ``precision="fp32c"``.  There is no CPU fallback: without the CUDA library or a B200
 the functions raise.
 
-Reference behaviours kept: probe sums skip pairs with r^2 <= 1e-8; self sums skip
+Host radii that are all equal select the library's uniform-core sweeps (same values, fewer
+operations).  Reference behaviours kept: probe sums skip pairs with r^2 <= 1e-8; self sums skip
 j == i and use the pair core (sigma_i + sigma_j)/2; PSE uses the target's viscosity;
 helicity and enstrophy keep the wrapper's extra 1/(4 pi) (``set_reference_scaling``
 turns it off).  Reference defects not kept: scalar accumulators start at zero (the
@@ -89,11 +90,29 @@ def _ret(t, mode):
         return t
     if t.dim() == 0:
         return float(t.item())
-    return t.cpu() if mode == "torch" else t.cpu().numpy()
+    if mode == "torch":
+        # host tensors in, host tensors out: copy into page-locked memory (the caching host
+        # allocator reuses it), which the copy engine fills at full PCIe/C2C speed
+        out = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        out.copy_(t, non_blocking=True)
+        torch.cuda.current_stream(t.device).synchronize()
+        return out
+    return t.cpu().numpy()
 
 
 def _prec(precision):
     return _state["precision"] if precision is None else precision
+
+
+def _uniform(radii):
+    """Host radii that are all equal select the uniform-core sweeps (same pair values, 2 FP32
+    operations fewer per pair); device radii are not inspected (that would need a sync)."""
+    if isinstance(radii, torch.Tensor):
+        if radii.is_cuda:
+            return False
+        radii = radii.numpy()
+    r = np.asarray(radii).reshape(-1)
+    return bool(r.size) and bool(np.all(r == r[0]))
 
 
 def get_induced_velocity_at(target_positions, particles_positions, particles_strengths,
@@ -105,8 +124,10 @@ def get_induced_velocity_at(target_positions, particles_positions, particles_str
 
 def get_selfinduced_velocity(particles_positions, particles_strengths, particles_radii,
                              precision=None):
+    uc = _uniform(particles_radii)
     (x, a, s), np_mode = _prep((particles_positions, particles_strengths, particles_radii))
-    return _ret(kernels.selfinduced_velocity(x, a, s, precision=_prec(precision)), np_mode)
+    return _ret(kernels.selfinduced_velocity(x, a, s, precision=_prec(precision),
+                                             uniform_core=uc), np_mode)
 
 
 def get_vorticity_field_at(target_positions, particle_positions, particle_strengths,
@@ -118,13 +139,17 @@ def get_vorticity_field_at(target_positions, particle_positions, particle_streng
 
 def get_strength_gradients(particle_positions, particle_strengths, particle_radii,
                            precision=None):
+    uc = _uniform(particle_radii)
     (x, a, s), np_mode = _prep((particle_positions, particle_strengths, particle_radii))
-    return _ret(kernels.strength_gradients(x, a, s, precision=_prec(precision)), np_mode)
+    return _ret(kernels.strength_gradients(x, a, s, precision=_prec(precision),
+                                           uniform_core=uc), np_mode)
 
 
 def get_strength_gradients_PSE(positions, strengths, radii, viscosities, precision=None):
+    uc = _uniform(radii)
     (x, a, s, v), np_mode = _prep((positions, strengths, radii, viscosities))
-    return _ret(kernels.strength_gradients_pse(x, a, s, v, precision=_prec(precision)), np_mode)
+    return _ret(kernels.strength_gradients_pse(x, a, s, v, precision=_prec(precision),
+                                               uniform_core=uc), np_mode)
 
 
 def get_total_kinetic_energy(particles_positions, particles_strengths, particles_radii,
@@ -142,14 +167,17 @@ def get_total_helicity(particles_positions, particles_strengths, particles_radii
 
 def get_total_enstrophy(particles_positions, particles_strengths, particles_radii,
                         precision=None):
+    uc = _uniform(particles_radii)
     (x, a, s), np_mode = _prep((particles_positions, particles_strengths, particles_radii))
     return _ret(kernels.total_enstrophy(x, a, s, ref_extra_4pi=_state["ref_extra_4pi"],
-                                        precision=_prec(precision)), np_mode)
+                                        precision=_prec(precision), uniform_core=uc), np_mode)
 
 
 def get_selfinduced_velocity_and_strength_gradients(particles_positions, particles_strengths,
                                                     particles_radii, precision=None):
     """Fused ``get_selfinduced_velocity`` + ``get_strength_gradients`` (one sweep)."""
+    uc = _uniform(particles_radii)
     (x, a, s), np_mode = _prep((particles_positions, particles_strengths, particles_radii))
-    u, g = kernels.velocity_and_strength_gradients(x, a, s, precision=_prec(precision))
+    u, g = kernels.velocity_and_strength_gradients(x, a, s, precision=_prec(precision),
+                                                   uniform_core=uc)
     return _ret(u, np_mode), _ret(g, np_mode)
