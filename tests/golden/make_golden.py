@@ -22,6 +22,8 @@ It executes the reference's own code and writes ``tests/golden/*.npz``:
 * ``ic.npz``           -- ``OpenONDA/utilities/vpm_flow_models.py`` (vortex_ring_vpm,
   lamb_oseen_vpm, isotropic_turbulence_vpm) and ``vpm_solver_helper.py`` (rectangular, 2-D rectangular, hexagonal and
   cylindrical lattices) on the seeded cases of ``ic_cases()``.
+* ``manage.npz``       -- the reference ParticleSystem's O(N) diagnostics, remove_weak_particles
+  (relative with circulation conservation, absolute) and get_highest_nonzero_indices.
 * ``step_ring8192.npz`` -- one DNS+PSE+RK4 step of the 8192-particle ring through the
   reference ``ParticleSystem`` sequencing with the GPU-semantics oracle kernels injected as
   its physics module (the simulator is too slow at this size).
@@ -412,6 +414,50 @@ def make_ic(ref):
     np.savez_compressed(os.path.join(HERE, "ic.npz"), **out)
 
 
+def manage_field():
+    f = configs.random_cloud(400, seed=31, nu=1e-3)
+    f.strengths *= np.random.default_rng(32).uniform(0.1, 3.0, size=(400, 1))
+    return f
+
+
+def make_manage(ref):
+    """Particle-field control and O(N) diagnostics of the reference ParticleSystem
+    (vpmModule.py:264-284, :970-1037, :1124-1166) on a seeded cloud."""
+    vpm = import_vpm_module(ref)
+    f = manage_field()
+    mags = np.linalg.norm(f.strengths, axis=1)
+    out = {"field/positions": f.positions, "field/strengths": f.strengths,
+           "field/radii": f.radii, "field/viscosities": f.viscosities}
+
+    def fresh():
+        ps = vpm.ParticleSystem(monitor_variables=[], backup_frequency=10 ** 9,
+                                processing_unit="CPU")
+        ps.add_particle_field(f.positions.copy(), np.zeros_like(f.positions),
+                              f.strengths.copy(), f.radii.copy(), f.viscosities.copy())
+        return ps
+
+    with contextlib.redirect_stdout(io.StringIO()):
+        ps = fresh()
+        out["diag/linear_impulse"] = ps.get_total_linear_impulse()
+        out["diag/angular_impulse"] = ps.get_total_angular_impulse()
+        out["diag/total_strength"] = ps.get_total_strength()
+        out["diag/total_strength_magnitude"] = np.array(ps.get_total_strength_magnitude())
+        cases = {"relative_conserve": ("relative", 0.4, True),
+                 "absolute": ("absolute", float(np.median(mags)), False)}
+        for name, (mode, thr, conserve) in cases.items():
+            ps = fresh()
+            ps.remove_weak_particles(mode, thr, conserve_total_circulation=conserve)
+            out[f"{name}/positions"] = ps.get_particle_positions()
+            out[f"{name}/strengths"] = ps.get_particle_strengths()
+            out[f"{name}/radii"] = ps.get_particle_radii()
+            out[f"{name}/threshold"] = np.array(thr)
+    out["highest/top10"] = vpm.get_highest_nonzero_indices(mags, top_percentage=10)
+    out["highest/above"] = vpm.get_highest_nonzero_indices(
+        mags, strength_threshold=float(np.percentile(mags, 80)))
+    out["highest/mags"] = mags
+    np.savez_compressed(os.path.join(HERE, "manage.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=DEFAULT_REF)
@@ -433,6 +479,7 @@ def main():
         "steps_gpu": make_steps_gpu,
         "step_ring8192": make_step_ring8192,
         "ic": make_ic,
+        "manage": make_manage,
     }
     only = set(args.only.split(",")) if args.only else set(jobs)
     for name, fn in jobs.items():

@@ -1,5 +1,6 @@
 """ParticleSystem host-side behaviour that needs no GPU: constructor validation with the
 reference's messages (vpmModule.py:117-184) and the LES/BDF constants."""
+import numpy as np
 import pytest
 
 from openonda_b200.vpm import vpmModule as v
@@ -37,3 +38,17 @@ def test_highest_nonzero_indices():
     a = np.array([0.0, 3.0, 1.0, 0.0, 2.0])
     assert list(v.get_highest_nonzero_indices(a, top_percentage=50)) == [1]
     assert list(v.get_highest_nonzero_indices(a, strength_threshold=1.5)) == [1, 4]
+
+
+def test_get_highest_nonzero_indices_matches_reference():
+    """vpmModule.get_highest_nonzero_indices (vpmModule.py:1124-1166) on the reference's own
+    output (tests/golden/manage.npz)."""
+    from conftest import golden
+    from openonda_b200.vpm.vpmModule import get_highest_nonzero_indices
+
+    g = golden("manage.npz")
+    mags = g["highest/mags"]
+    assert np.array_equal(get_highest_nonzero_indices(mags, top_percentage=10), g["highest/top10"])
+    thr = float(np.percentile(mags, 80))
+    assert np.array_equal(get_highest_nonzero_indices(mags, strength_threshold=thr),
+                          g["highest/above"])
