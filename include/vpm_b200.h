@@ -1,9 +1,13 @@
 /*
  * vpm_b200.h -- C ABI of the B200 (sm_100a) VPM pair-sum library (libvpm_b200.so).
  *
- * Every compute entry point replaces one module-level function of OpenONDA's Numba-CUDA
+ * The pair-sum entry points replace the module-level functions of OpenONDA's Numba-CUDA
  * physics module, OpenONDA/solvers/VPM/ParticlesPhysicsCuda.py, which
- * vpmModule.ParticleSystem selects in _load_physics_module (vpmModule.py:141-154).
+ * vpmModule.ParticleSystem selects in _load_physics_module (vpmModule.py:141-154).  The
+ * element-wise step kernels restate vpmModule.ParticleSystem's updates, and the
+ * initial-condition entry points OpenONDA/utilities/vpm_flow_models.py and
+ * vpm_solver_helper.py.  The fused sums, the adjoint, the uniform-core flag and the
+ * no-allocation variant have no counterpart in the reference (each says so).
  *
  * Conventions
  *   - Arrays are DEVICE pointers in the reference's layout: positions, strengths and

@@ -1,10 +1,12 @@
-// vpm_abi.cu -- C-ABI entry points, launch planning, pack and finalize kernels.
+// vpm_abi.cu -- C-ABI entry points, launch planning, pack and finalize kernels.  The
+// library is one translation unit: the step, reference-algorithm and initial-condition
+// kernels are included at the end.
 //
-// One call = pack (reference AoS float64 -> packed records in the compute precision,
-// inside the caller's workspace) -> tiled sweep (partials per source split, FP64) ->
-// finalize (sum the splits in order, apply target-only factors, write the reference's
-// output layout).  Scalars reduce the per-target values in a single block in a fixed
-// order, so every result is deterministic.
+// One pair-sum call = pack (reference AoS float64 -> packed records in the compute
+// precision, inside the caller's workspace) -> tiled sweep (partials per source split,
+// FP64) -> finalize (sum the splits in order, apply target-only factors, write the
+// reference's output layout).  Scalars reduce the per-target values in a single block in a
+// fixed order, so every result is deterministic.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
