@@ -55,9 +55,16 @@ struct Cfg<float2> {
   static constexpr int R = VPM_FP32_R, THREADS = VPM_FP32_THREADS, TILE = 256, STAGES = 2,
                        MINB = VPM_FP32_MINB;
 };
+#ifndef VPM_FP64_R
+#define VPM_FP64_R 1
+#endif
+#ifndef VPM_FP64_THREADS
+#define VPM_FP64_THREADS 128
+#endif
 template <>
 struct Cfg<double> {
-  static constexpr int R = 2, THREADS = 128, TILE = 128, STAGES = 2, MINB = 1;
+  static constexpr int R = VPM_FP64_R, THREADS = VPM_FP64_THREADS, TILE = 128, STAGES = 2,
+                       MINB = 1;
 };
 
 constexpr int kMaxSplits = 64;
