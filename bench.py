@@ -457,6 +457,11 @@ def main():
                          "fp32_pipe_frac": round(achieved / peak * 2 * FP32_OPS_PER_PAIR_FUSED
                                                  / FLOPS_PER_PAIR_FUSED, 4),
                          "packed_ffma2_peak": round(ffma2_peak, 3),
+                         # FP32 lane-ops (x2, the FMA flop convention) against the packed-FFMA2
+                         # microbenchmark: the ceiling of this instruction mix
+                         "fp32_pipe_frac_of_packed_peak": round(
+                             achieved / ffma2_peak * 2 * FP32_OPS_PER_PAIR_FUSED
+                             / FLOPS_PER_PAIR_FUSED, 4),
                          "sfu": {"rsqrt_per_pair": 1,
                                  "achieved_t_per_s": round(pairs_per_launch / t_sweep / 1e12,
                                                            4),

@@ -67,8 +67,14 @@ struct Cfg<double> {
                        MINB = 1;
 };
 
-constexpr int kMaxSplits = 64;
-constexpr int64_t kMinChunk = 256;
+#ifndef VPM_MAX_SPLITS
+#define VPM_MAX_SPLITS 64
+#endif
+#ifndef VPM_MIN_CHUNK
+#define VPM_MIN_CHUNK 256
+#endif
+constexpr int kMaxSplits = VPM_MAX_SPLITS;
+constexpr int64_t kMinChunk = VPM_MIN_CHUNK;
 constexpr size_t kMaxPartialBytes = size_t(4) << 30;
 
 struct Plan {
