@@ -66,10 +66,12 @@ class RHS(torch.autograd.Function):
     """(u, S [+ P]) with a hand-written vector-Jacobian product."""
 
     @staticmethod
-    def forward(ctx, x, a, sigma, nu, precision, with_pse):
-        u, rate = kernels.velocity_and_strength_gradients(x, a, sigma, precision=precision)
+    def forward(ctx, x, a, sigma, nu, precision, with_pse, uniform_core=False):
+        u, rate = kernels.velocity_and_strength_gradients(x, a, sigma, precision=precision,
+                                                          uniform_core=uniform_core)
         if with_pse:
-            rate = rate + kernels.strength_gradients_pse(x, a, sigma, nu, precision=precision)
+            rate = rate + kernels.strength_gradients_pse(x, a, sigma, nu, precision=precision,
+                                                         uniform_core=uniform_core)
         ctx.save_for_backward(x, a, sigma, nu if with_pse else None)
         ctx.precision, ctx.with_pse = precision, with_pse
         return u, rate
@@ -83,7 +85,7 @@ class RHS(torch.autograd.Function):
             grad_rate = torch.zeros_like(a)
         gx, ga, gs, gnu = rhs_vjp(x, a, sigma, nu if ctx.with_pse else None,
                                   grad_u.contiguous(), grad_rate.contiguous(), ctx.precision)
-        return gx, ga, gs, gnu, None, None
+        return gx, ga, gs, gnu, None, None, None
 
 
 class KineticEnergy(torch.autograd.Function):
@@ -102,23 +104,25 @@ class KineticEnergy(torch.autograd.Function):
         return gx * grad_e, ga * grad_e, gs * grad_e, None
 
 
-def rhs(x, a, sigma, nu=None, precision="fp64"):
-    """Differentiable (u, dalpha/dt); PSE is included when ``nu`` is given."""
+def rhs(x, a, sigma, nu=None, precision="fp64", uniform_core=False):
+    """Differentiable (u, dalpha/dt); PSE is included when ``nu`` is given.  With
+    ``uniform_core`` (all cores equal) the forward sums take the uniform-core form."""
     with_pse = nu is not None
     return RHS.apply(x, a, sigma, nu if with_pse else torch.zeros_like(sigma), precision,
-                     with_pse)
+                     with_pse, bool(uniform_core))
 
 
 def kinetic_energy(x, a, sigma, precision="fp64"):
     return KineticEnergy.apply(x, a, sigma, precision)
 
 
-def rk4_step(x, a, sigma, nu, dt, precision="fp64"):
+def rk4_step(x, a, sigma, nu, dt, precision="fp64", uniform_core=False):
     """One classical RK4 step of (x, alpha) with frozen sigma and nu."""
-    k1x, k1a = rhs(x, a, sigma, nu, precision)
-    k2x, k2a = rhs(x + (dt / 2) * k1x, a + (dt / 2) * k1a, sigma, nu, precision)
-    k3x, k3a = rhs(x + (dt / 2) * k2x, a + (dt / 2) * k2a, sigma, nu, precision)
-    k4x, k4a = rhs(x + dt * k3x, a + dt * k3a, sigma, nu, precision)
+    uc = uniform_core
+    k1x, k1a = rhs(x, a, sigma, nu, precision, uc)
+    k2x, k2a = rhs(x + (dt / 2) * k1x, a + (dt / 2) * k1a, sigma, nu, precision, uc)
+    k3x, k3a = rhs(x + (dt / 2) * k2x, a + (dt / 2) * k2a, sigma, nu, precision, uc)
+    k4x, k4a = rhs(x + dt * k3x, a + dt * k3a, sigma, nu, precision, uc)
     x1 = x + (dt / 6) * (k1x + 2 * k2x + 2 * k3x + k4x)
     a1 = a + (dt / 6) * (k1a + 2 * k2a + 2 * k3a + k4a)
     return x1, a1
@@ -129,12 +133,15 @@ def trajectory(x0, a0, sigma, nu=None, dt=0.01, steps=10, precision="fp64",
     """Integrate ``steps`` RK4 steps; differentiable w.r.t. x0, a0, sigma (and nu).
 
     With autograd active, every segment of ``checkpoint_every`` steps is recomputed in the
-    backward pass (only segment-start states are stored)."""
+    backward pass (only segment-start states are stored).  sigma is frozen along the
+    trajectory, so equal cores (checked once) select the uniform-core forward sums."""
     x, a = x0, a0
+    with torch.no_grad():
+        uc = sigma.numel() > 0 and bool((sigma == sigma.reshape(-1)[0]).all())
 
     def segment(xs, as_, sig, visc, n_steps):
         for _ in range(n_steps):
-            xs, as_ = rk4_step(xs, as_, sig, visc, dt, precision)
+            xs, as_ = rk4_step(xs, as_, sig, visc, dt, precision, uc)
         return xs, as_
 
     done = 0

@@ -130,8 +130,11 @@ struct Sweep {
   using RecT = typename Op::Record;
   static constexpr int NV = Op::NV;
   static constexpr int R = Op::kR ? Op::kR : C::R;
-  // the same tile bytes for every record width
-  static constexpr int TILE = int(C::TILE * sizeof(Rec<T>) / sizeof(RecT));
+  // about the same tile bytes for every record width; FP32 tiles hold whole carry windows
+  static constexpr int kTileRaw = int(C::TILE * sizeof(Rec<T>) / sizeof(RecT));
+  static constexpr int TILE =
+      LaneTraits<T>::kLanes == 2 ? kTileRaw / kCarryWindow * kCarryWindow : kTileRaw;
+  static_assert(TILE >= kCarryWindow || LaneTraits<T>::kLanes == 1, "tile below a window");
   static constexpr size_t kSmem =
       sweep_smem_bytes<T, RecT, Op::NV, R, C::THREADS, TILE, C::STAGES>();
   static void* kernel() {
@@ -386,11 +389,18 @@ __global__ void pack_grad_kernel(const double* __restrict__ pos, const double* _
   set_elem(r.ux, -kOneOver4Pi * gu[3 * i]);
   set_elem(r.uy, -kOneOver4Pi * gu[3 * i + 1]);
   set_elem(r.uz, -kOneOver4Pi * gu[3 * i + 2]);
+  const double ax = str[3 * i], ay = str[3 * i + 1], az = str[3 * i + 2];
+  const double sx = kOneOver4Pi * gs[3 * i], sy = kOneOver4Pi * gs[3 * i + 1],
+               sz = kOneOver4Pi * gs[3 * i + 2];
+  set_elem(r.gx, sx);
+  set_elem(r.gy, sy);
+  set_elem(r.gz, sz);
+  set_elem(r.mx, ay * sz - az * sy);  // m = a x s'
+  set_elem(r.my, az * sx - ax * sz);
+  set_elem(r.mz, ax * sy - ay * sx);
   set_elem(r.pad0, 0.0);
-  set_elem(r.gx, kOneOver4Pi * gs[3 * i]);
-  set_elem(r.gy, kOneOver4Pi * gs[3 * i + 1]);
-  set_elem(r.gz, kOneOver4Pi * gs[3 * i + 2]);
   set_elem(r.pad1, 0.0);
+  set_elem(r.pad2, 0.0);
   out[i] = r;
 }
 

@@ -36,19 +36,21 @@
 
 namespace vpm {
 
-// Wide record: state plus pre-scaled cotangents (128 bytes for both element types).
+// Wide record: state, pre-scaled cotangents and the per-particle product m = a x s'
+// (160 bytes for both element types; m is formed in FP64 by the pack kernel).
 template <class E>
 struct alignas(16) RecG {
   E x, y, z, s;
-  E ax, ay, az, nu;     // nu holds 105 * nu
-  E ux, uy, uz, pad0;   // -ubar / (4 pi)
-  E gx, gy, gz, pad1;   // sbar / (4 pi)
+  E ax, ay, az, nu;    // nu holds 105 * nu
+  E ux, uy, uz, mx;    // -ubar / (4 pi); m = a x s'
+  E gx, gy, gz, my;    // sbar / (4 pi)
+  E mz, pad0, pad1, pad2;
 };
-static_assert(sizeof(RecG<double>) == 128 && sizeof(RecG<float2>) == 128, "RecG is 128 B");
+static_assert(sizeof(RecG<double>) == 160 && sizeof(RecG<float2>) == 160, "RecG is 160 B");
 
 template <class V>
 struct SrcG {
-  V x, y, z, s, ax, ay, az, nu, ux, uy, uz, gx, gy, gz;
+  V x, y, z, s, ax, ay, az, nu, ux, uy, uz, gx, gy, gz, mx, my, mz;
 };
 
 template <class V>
@@ -58,17 +60,21 @@ struct TgtG {
 
 __device__ __forceinline__ SrcG<double> load_srcg(const RecG<double>& r) {
   const double2* p = reinterpret_cast<const double2*>(&r);
-  const double2 a = p[0], b = p[1], c = p[2], d = p[3], e = p[4], f = p[5], g = p[6], h = p[7];
-  return SrcG<double>{a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x, e.y, f.x, g.x, g.y, h.x};
+  const double2 a = p[0], b = p[1], c = p[2], d = p[3], e = p[4], f = p[5], g = p[6], h = p[7],
+                i = p[8];
+  return SrcG<double>{a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x, e.y, f.x,
+                      g.x, g.y, h.x, f.y, h.y, i.x};
 }
 __device__ __forceinline__ SrcG<float2> load_srcg(const RecG<float2>& r) {
   const float4* p = reinterpret_cast<const float4*>(&r);
-  const float4 a = p[0], b = p[1], c = p[2], d = p[3], e = p[4], f = p[5], g = p[6], h = p[7];
+  const float4 a = p[0], b = p[1], c = p[2], d = p[3], e = p[4], f = p[5], g = p[6], h = p[7],
+               i = p[8];
   return SrcG<float2>{make_float2(a.x, a.y), make_float2(a.z, a.w), make_float2(b.x, b.y),
                       make_float2(b.z, b.w), make_float2(c.x, c.y), make_float2(c.z, c.w),
                       make_float2(d.x, d.y), make_float2(d.z, d.w), make_float2(e.x, e.y),
                       make_float2(e.z, e.w), make_float2(f.x, f.y), make_float2(g.x, g.y),
-                      make_float2(g.z, g.w), make_float2(h.x, h.y)};
+                      make_float2(g.z, g.w), make_float2(h.x, h.y), make_float2(f.z, f.w),
+                      make_float2(h.z, h.w), make_float2(i.x, i.y)};
 }
 
 __device__ __forceinline__ TgtG<double> make_tgtg(const RecG<double>* const* r) {
@@ -185,9 +191,9 @@ struct OpRhsVjp {
     acc[VJ_GU + 1] = fma(g, s.uy, acc[VJ_GU + 1]);
     acc[VJ_GU + 2] = fma(g, s.uz, acc[VJ_GU + 2]);
     // abar: g (r x u'_l - a_l x s'_l) + f dp (r x a_l); the G_a x s'_k part is in finalize
-    const V nx = fma(ry, s.uz, -(rz * s.uy)) - fma(s.ay, s.gz, -(s.az * s.gy));
-    const V ny = fma(rz, s.ux, -(rx * s.uz)) - fma(s.az, s.gx, -(s.ax * s.gz));
-    const V nz = fma(rx, s.uy, -(ry * s.ux)) - fma(s.ax, s.gy, -(s.ay * s.gx));
+    const V nx = fma(ry, s.uz, -(rz * s.uy)) - s.mx;  // m_l = a_l x s'_l from the record
+    const V ny = fma(rz, s.ux, -(rx * s.uz)) - s.my;
+    const V nz = fma(rx, s.uy, -(ry * s.ux)) - s.mz;
     acc[VJ_A + 0] = fma(g, nx, fma(fdp, clx, acc[VJ_A + 0]));
     acc[VJ_A + 1] = fma(g, ny, fma(fdp, cly, acc[VJ_A + 1]));
     acc[VJ_A + 2] = fma(g, nz, fma(fdp, clz, acc[VJ_A + 2]));
