@@ -249,6 +249,12 @@ def config5(args):
             _step(ps)
         t_total += t.ms
     eu, eg = _errors_vs_fp64(ps)
+    # the LES filter sums of the final state, FP32c against FP64 (same FP32-rounded state)
+    x32, a32, s32 = (t.float().double() for t in (ps.positions, ps.strengths, ps.radii))
+    les64 = kernels.les_step_sums(x32, a32, s32, precision="fp64")
+    les32 = kernels.les_step_sums(x32, a32, s32, precision="fp32c", uniform_core=ps._uc)
+    ew = _rel(les32[2], les64[2])
+    ee = abs(float(les32[3]) - float(les64[3])) / abs(float(les64[3]))
     n = f.n
     # 7 N^2 pair sums per step as the reference counts them (velocity + stretching counted
     # once), run here as 5 sweeps: LES step sums (velocity, stretching, vorticity,
@@ -260,6 +266,7 @@ def config5(args):
            "pair_sums_per_step": int(sums), "sweeps_per_step": 5,
            "gpairs_per_s": round(sums * n * n / (t_total / steps / 1e3) / 1e9, 1),
            "rel_err_velocity_last_step": eu, "rel_err_stretching_last_step": eg,
+           "rel_err_vorticity_last_step": ew, "rel_err_enstrophy_last_step": ee,
            "cnu": ps.Cnu})
 
 
