@@ -31,10 +31,15 @@ sys.path.insert(0, HERE)
 
 METRIC = "Biot-Savart Gpairs/s at N=1M: FP32-compensated vs FP64 at <=1e-6 rel err"
 UNIT = "Gpairs/s"
-# FP32-pipe work per pair of the fused velocity + stretching sweep:
-# 38 FP32 lane-ops = 19 FFMA + 12 FMUL + 7 FADD -> 57 flops (FMA = 2), 1 MUFU.RSQ.
+# FP32-pipe work per ordered pair of the fused velocity + stretching sweep.
+# One-sided: 38 FP32 lane-ops = 19 FFMA + 12 FMUL + 7 FADD -> 57 flops (FMA = 2), 1 MUFU.RSQ.
+# Both-sides (each unordered pair once for both particles): 53 lane-ops = 31 FFMA + 15 FMUL
+# + 7 FADD -> 84 flops and 1 MUFU per unordered pair, i.e. 26.5 lane-ops, 42 flops and 0.5
+# MUFU per ordered pair.
 FLOPS_PER_PAIR_FUSED = 57
 FP32_OPS_PER_PAIR_FUSED = 38
+FLOPS_PER_PAIR_BOTH = 42
+FP32_OPS_PER_PAIR_BOTH = 26.5
 L2_FLUSH_BYTES = 512 << 20
 
 
@@ -424,11 +429,18 @@ def main():
 
     if rank == 0:
         pairs_per_launch = float(m_local) * n
-        achieved = FLOPS_PER_PAIR_FUSED * pairs_per_launch / t_sweep / 1e12
+        both = sweep32.both_sides
+        flops_pp = FLOPS_PER_PAIR_BOTH if both else FLOPS_PER_PAIR_FUSED
+        ops_pp = FP32_OPS_PER_PAIR_BOTH if both else FP32_OPS_PER_PAIR_FUSED
+        rsqrt_pp = 0.5 if both else 1.0
+        achieved = flops_pp * pairs_per_launch / t_sweep / 1e12
         traffic = load_traffic()
         tr = None
-        if traffic and traffic.get("kernel_traffic_bytes_per_particle") is not None:
-            # DRAM traffic of the sweep grows with the particle count, not with N^2
+        if traffic and both and traffic.get("both_sides"):
+            # both-sides sweep: accumulator read-modify-writes per tile pair, ~N^2
+            tr = round(traffic["both_sides"]["bytes_per_pair"] * float(m_local) * n)
+        elif traffic and traffic.get("kernel_traffic_bytes_per_particle") is not None:
+            # one-sided sweep: DRAM traffic grows with the particle count, not with N^2
             tr = round(traffic["kernel_traffic_bytes_per_particle"] * n)
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
@@ -453,21 +465,21 @@ def main():
                          "peak": round(peak, 3), "unit": "TFLOP/s",
                          "frac": round(achieved / peak, 4), "traffic": tr,
                          "peak_source": "FFMA microbenchmark measured in this run",
-                         "flops_per_pair": FLOPS_PER_PAIR_FUSED,
-                         "fp32_pipe_frac": round(achieved / peak * 2 * FP32_OPS_PER_PAIR_FUSED
-                                                 / FLOPS_PER_PAIR_FUSED, 4),
+                         "kernel": ("both-sides sweep, " if both else "one-sided sweep, ")
+                                   + f"{sweep32.sweep_launches} launches per call",
+                         "flops_per_pair": flops_pp,
+                         "fp32_pipe_frac": round(achieved / peak * 2 * ops_pp / flops_pp, 4),
                          "packed_ffma2_peak": round(ffma2_peak, 3),
                          # FP32 lane-ops (x2, the FMA flop convention) against the packed-FFMA2
                          # microbenchmark: the ceiling of this instruction mix
                          "fp32_pipe_frac_of_packed_peak": round(
-                             achieved / ffma2_peak * 2 * FP32_OPS_PER_PAIR_FUSED
-                             / FLOPS_PER_PAIR_FUSED, 4),
-                         "sfu": {"rsqrt_per_pair": 1,
-                                 "achieved_t_per_s": round(pairs_per_launch / t_sweep / 1e12,
-                                                           4),
+                             achieved / ffma2_peak * 2 * ops_pp / flops_pp, 4),
+                         "sfu": {"rsqrt_per_pair": rsqrt_pp,
+                                 "achieved_t_per_s": round(
+                                     rsqrt_pp * pairs_per_launch / t_sweep / 1e12, 4),
                                  "peak_t_per_s": round(sfu_peak, 4),
-                                 "frac": round(pairs_per_launch / t_sweep / 1e12 / sfu_peak,
-                                               4),
+                                 "frac": round(rsqrt_pp * pairs_per_launch / t_sweep / 1e12
+                                               / sfu_peak, 4),
                                  "peak_source": "MUFU rsqrt microbenchmark in this run"}},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},

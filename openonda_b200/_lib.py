@@ -62,6 +62,8 @@ SIGNATURES = {
     "vpm_total_helicity": ([_P, _P, _P, _I64, _I, _P, _I, _P, _SZ, _P], _I),
     "vpm_total_enstrophy": ([_P, _P, _P, _I64, _I, _P, _I, _P, _SZ, _P], _I),
     "vpm_velocity_and_strength_gradients": ([_P, _P, _P, _I64, _P, _P, _I, _P, _SZ, _P], _I),
+    "vpm_set_symmetric_min_n": ([_I64], _I64),
+    "vpm_sweep_launches": ([_I, _I, _I64, _I64], _I64),
     "vpm_les_step_sums": ([_P, _P, _P, _I64, _P, _P, _P, _P, _I, _I, _P, _SZ, _P], _I),
     "vpm_rhs_vjp": ([_P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _I, _P, _SZ, _P], _I),
     "vpm_kinetic_energy_grad": ([_P, _P, _P, _I64, _P, _P, _P, _I, _P, _SZ, _P], _I),

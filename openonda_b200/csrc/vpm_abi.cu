@@ -7,6 +7,7 @@
 // FP64) -> finalize (sum the splits in order, apply target-only factors, write the
 // reference's output layout).  Scalars reduce the per-target values in a single block in a
 // fixed order, so every result is deterministic.
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -19,6 +20,7 @@
 #include "vpm_b200.h"
 #include "vpm_sweep.cuh"
 #include "vpm_adjoint.cuh"
+#include "vpm_rot.cuh"
 
 namespace vpm {
 namespace {
@@ -79,13 +81,18 @@ constexpr size_t kMaxPartialBytes = size_t(4) << 30;
 
 struct Plan {
   int64_t tblocks = 0;
-  int splits = 1;
+  int splits = 1;  // source splits; the both-sides sweep: its accumulator sets (4 per pair)
   int64_t chunk = 0;
   size_t smem = 0;
   int threads = 0;
   int r = 0;
   int nv = 0;
+  int pairs = 0;  // both-sides sweep (vpm_rot.cuh): diagonal pairs per launch; 0 = one-sided
 };
+
+// FP32 self sums of velocity + stretching with at least this many particles evaluate each
+// unordered pair once for both particles (vpm_set_symmetric_min_n changes it).
+std::atomic<int64_t> g_sym_min_n{int64_t(1) << 17};
 
 struct DevInfo {
   int sms = 0;
@@ -369,6 +376,99 @@ int zero_out(double* p, int64_t count, cudaStream_t st) {
   return VPM_OK;
 }
 
+// Both-sides sweep of the FP32 fused self sum (vpm_rot.cuh): launch 0 on the diagonal tiles,
+// then ceil(floor(nt/2) / m) launches of m diagonal pairs each.
+template <class Op>
+struct RotSweep {
+  static constexpr int NV = Op::NV;
+  static constexpr int kMaxPairs = 8;
+  static constexpr size_t kSmem = rot_smem_bytes();
+  static int64_t tiles(int64_t n) { return (n + kRotTile - 1) / kRotTile; }
+
+  // Shared-memory attributes and resident CTAs per SM, once per device (cached like the
+  // one-sided sweeps' plans).
+  static int prepare(int* occ) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    const void* ks = reinterpret_cast<const void*>(&rot_sweep_kernel<Op, false>);
+    const void* kd = reinterpret_cast<const void*>(&rot_sweep_kernel<Op, true>);
+    const auto key = std::make_pair(ks, dev);
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_occ.find(key);
+    if (it != g_occ.end()) {
+      *occ = it->second;
+      return VPM_OK;
+    }
+    for (const void* fn : {kd, ks}) {
+      e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmem));
+      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(both-sides sweep)");
+    }
+    int o = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, ks, kRotThreads, kSmem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    *occ = o > 0 ? o : 1;
+    g_occ[key] = *occ;
+    return VPM_OK;
+  }
+
+  static int plan(int64_t n, Plan* p) {
+    DevInfo d;
+    int rc = device_info(&d);
+    if (rc) return rc;
+    int occ = 1;
+    rc = prepare(&occ);
+    if (rc) return rc;
+    const int64_t nt = tiles(n);
+    const int64_t npairs = nt / 2;
+    const double slots = double(d.sms) * occ;
+    // pairs per launch: the first m (from 1) whose m * nt CTAs fill 97 % of whole waves,
+    // else the best one up to kMaxPairs
+    int best_m = 1;
+    double best = -1.0;
+    for (int m = 1; m <= kMaxPairs && m <= npairs; ++m) {
+      const double waves = double(m) * nt / slots;
+      const double eff = waves / std::ceil(waves);
+      if (eff > best + 1e-9) {
+        best = eff;
+        best_m = m;
+      }
+      if (eff >= 0.97) break;
+    }
+    p->pairs = best_m;
+    p->tblocks = nt;
+    p->splits = 4 * best_m;
+    p->chunk = n;
+    p->smem = kSmem;
+    p->threads = kRotThreads;
+    p->r = 4;
+    p->nv = NV;
+    return VPM_OK;
+  }
+
+  // acc: [4 * pairs][NV][n] FP64, zeroed here.
+  static int launch(const Plan& p, const Rec<float2>* rec, int64_t n, double* acc,
+                    cudaStream_t st) {
+    const int nt = int(tiles(n));
+    int occ = 1;
+    int rc = prepare(&occ);
+    if (!rc) rc = zero_out(acc, int64_t(p.splits) * NV * n, st);
+    if (rc) return rc;
+    rot_sweep_kernel<Op, true><<<nt, kRotThreads, kSmem, st>>>(RotArgs{rec, n, nt, 0, acc});
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
+    const int npairs = nt / 2;
+    for (int k0 = 1; k0 <= npairs; k0 += p.pairs) {
+      const int m = (npairs - k0 + 1 < p.pairs) ? npairs - k0 + 1 : p.pairs;
+      rot_sweep_kernel<Op, false><<<m * nt, kRotThreads, kSmem, st>>>(RotArgs{rec, n, nt, k0,
+                                                                              acc});
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
+    }
+    return VPM_OK;
+  }
+};
+
 // ---- adjoint: pack, finalize --------------------------------------------------------------
 template <class E>
 __global__ void pack_grad_kernel(const double* __restrict__ pos, const double* __restrict__ str,
@@ -471,6 +571,7 @@ struct Ops {
   using Ens = OpEns<T, REFINE, UC>;
   using VelStretch = OpVelStretch<T, REFINE, UC>;
   using LesStep = OpLesStep<T, REFINE, UC>;
+  using VelStretchBoth = OpVelStretchBoth<REFINE, UC>;  // FP32 only
   using RhsVjp = OpRhsVjp<T, REFINE, false>;
   using RhsVjpPse = OpRhsVjp<T, REFINE, true>;
   using KeGrad = OpKeGrad<T, REFINE>;
@@ -498,6 +599,11 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
     case VPM_OP_TOTAL_ENSTROPHY:
       return Sweep<typename O::Ens, T>::plan(m, n, p, mpb);
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
+      if constexpr (LaneTraits<T>::kLanes == 2) {
+        if (m == n && n >= g_sym_min_n.load() &&
+            RotSweep<typename O::VelStretchBoth>::tiles(n) >= 2)
+          return RotSweep<typename O::VelStretchBoth>::plan(n, p);
+      }
       return Sweep<typename O::VelStretch, T>::plan(m, n, p, mpb);
     case VPM_OP_LES_STEP_SUMS:
       return Sweep<typename O::LesStep, T>::plan(m, n, p, mpb);
@@ -634,7 +740,16 @@ int run(const Call& c) {
       if (!rc) rc = finalize_vec<T, FIN_PSE, 3>(part, p.splits, c.m, tgt, c.out, nullptr, c.st);
       return rc;
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
-      rc = Sweep<typename O::VelStretch, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+      if constexpr (LaneTraits<T>::kLanes == 2) {
+        if (p.pairs)  // m == n: the targets are all the records (tgt_begin == 0)
+          rc = RotSweep<typename O::VelStretchBoth>::launch(p, src, c.n, part, c.st);
+        else
+          rc = Sweep<typename O::VelStretch, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n,
+                                                        part, c.st);
+      } else {
+        rc = Sweep<typename O::VelStretch, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part,
+                                                      c.st);
+      }
       if (!rc)
         rc = finalize_vec<T, FIN_VELSTRETCH, O::VelStretch::NV>(part, p.splits, c.m, tgt, c.out,
                                                                c.out2, c.st);
@@ -1080,6 +1195,25 @@ int vpm_velocity_and_strength_gradients(const double* positions, const double* s
          nullptr, n, velocities, dalpha_dt, 0, workspace, workspace_bytes,
          static_cast<cudaStream_t>(stream)};
   return dispatch(c, precision);
+}
+
+int64_t vpm_set_symmetric_min_n(int64_t n) { return g_sym_min_n.exchange(n); }
+
+int64_t vpm_sweep_launches(int op, int precision, int64_t m, int64_t n) {
+  if (m <= 0 || n <= 0) return 0;
+  if (op == VPM_OP_RHS_VJP || op == VPM_OP_RHS_VJP_PSE || op == VPM_OP_KINETIC_ENERGY_GRAD)
+    precision &= ~VPM_UNIFORM_CORE;
+  Plan p;
+  const int rc = with_precision(precision, [&](auto P) {
+    using Pp = decltype(P);
+    return plan_op<typename Pp::type, Pp::refine, Pp::uc>(op, m, n, &p);
+  });
+  if (rc) return -1;
+  if (p.pairs) {  // zero the accumulators, the diagonal tiles, the diagonal-pair launches, finalize
+    const int64_t npairs = p.tblocks / 2;
+    return 3 + (npairs + p.pairs - 1) / p.pairs;
+  }
+  return 2;  // sweep, finalize (or the single-block reduction of a scalar)
 }
 
 int vpm_les_step_sums(const double* positions, const double* strengths, const double* radii,

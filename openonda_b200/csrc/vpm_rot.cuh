@@ -1,0 +1,242 @@
+// vpm_rot.cuh -- both-sides sweep of the fused velocity + stretching self sum, FP32-
+// compensated, with the source side carried around the warp in registers.
+//
+// The pair terms of (i <- j) and (j <- i) share r^2, the core, the rsqrt, g and f.  Seen from
+// particle j, with r = x_i - x_j as computed for target i:
+//   U_j += -g (r x a_i),   A_j += -g (a_j - a_i),   B_j += -h r,   h = f a_i . (r x a_j)
+// so one evaluation of an unordered pair costs 53 FP32 lane-ops instead of 2 x 38.
+//
+// Warp layout: each lane holds four targets (two packed FP32x2 lanes) and one source of the
+// current batch of 32 (read from L2, the next batch prefetched).  In 32 steps every lane meets
+// every source of the batch: after each step the sources and their source-side accumulators
+// move one lane down (__shfl_sync), so after the 32nd step each source is back in its lane
+// with its sums over the warp's 128 targets.  Warp shuffles are the second-scarcest resource
+// here (about one per two clocks per SM); four targets per lane keep them at 25 per 256
+// ordered pairs.  The source-side sums are then added over the CTA's warps in FP64 (fixed
+// order) and read-modify-written into the accumulator of the source particle.
+//
+// Tile-pair schedule (deterministic without atomics): particles form nt tiles of
+// T = 128 * WARPS.  A CTA owns one tile pair (I, J), I < J.  Diagonal pair q of a launch is
+// J - I = k (accumulator sets 4q / 4q+1 for the target / source side) together with
+// J - I = nt - k (sets 4q+2 / 4q+3): every (set, tile) is written by one CTA per launch, and
+// the launches run in stream order.  A launch runs m consecutive diagonal pairs (m chosen so
+// that its m * nt CTAs fill whole waves); launch 0 runs the diagonal tiles (I, I) one-sided
+// into set 0.  The finalize pass sums the 4m sets in order.
+//
+// Accumulation: target side in FP32 per batch of 32 sources, folded into FP64 carries held in
+// shared memory; source side in FP32 over the warp's 128 targets (each half of the packed
+// accumulator sums 64 terms), then FP64 across warps and tile pairs.
+#pragma once
+
+#include "vpm_sweep.cuh"
+
+namespace vpm {
+
+// Fused velocity + stretching, both sides of the pair (FP32x2 lanes).
+template <bool REFINE, bool UC>
+struct OpVelStretchBoth {
+  using V = float2;
+  using OneSided = OpVelStretch<float2, REFINE, UC>;
+  static constexpr int NV = 9;
+  __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
+                                               const Src<V>& s) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    V sg, s2;
+    pair_core<UC>(t, s, sg, s2);
+    const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
+    const V y = rsqrt_lane<REFINE>(x);
+    const V y2 = y * y;
+    const V y5 = (y2 * y2) * y;
+    const V t1 = fma(splat<V>(1.5), s2, x);
+    const V g = t1 * y5;
+    const V f = (t1 + s2) * (y5 * y2);
+    const V cx = fma(ry, s.az, -(rz * s.ay));
+    const V cy = fma(rz, s.ax, -(rx * s.az));
+    const V cz = fma(rx, s.ay, -(ry * s.ax));
+    acc[0] = fma(g, cx, acc[0]);
+    acc[1] = fma(g, cy, acc[1]);
+    acc[2] = fma(g, cz, acc[2]);
+    const V dx = s.ax - t.ax, dy = s.ay - t.ay, dz = s.az - t.az;
+    acc[3] = fma(g, dx, acc[3]);
+    acc[4] = fma(g, dy, acc[4]);
+    acc[5] = fma(g, dz, acc[5]);
+    const V h = f * fma(t.ax, cx, fma(t.ay, cy, t.az * cz));
+    acc[6] = fma(h, rx, acc[6]);
+    acc[7] = fma(h, ry, acc[7]);
+    acc[8] = fma(h, rz, acc[8]);
+    // source side, accumulated with the opposite sign (negated when it is stored)
+    const V ex = fma(ry, t.az, -(rz * t.ay));  // r x a_i
+    const V ey = fma(rz, t.ax, -(rx * t.az));
+    const V ez = fma(rx, t.ay, -(ry * t.ax));
+    jv[0] = fma(g, ex, jv[0]);
+    jv[1] = fma(g, ey, jv[1]);
+    jv[2] = fma(g, ez, jv[2]);
+    jv[3] = fma(g, dx, jv[3]);
+    jv[4] = fma(g, dy, jv[4]);
+    jv[5] = fma(g, dz, jv[5]);
+    jv[6] = fma(h, rx, jv[6]);
+    jv[7] = fma(h, ry, jv[7]);
+    jv[8] = fma(h, rz, jv[8]);
+  }
+};
+
+struct RotArgs {
+  const Rec<float2>* rec;  // packed records of all n particles
+  int64_t n;
+  int nt;       // tiles of kRotTile particles
+  int k0;       // first diagonal of this launch (0 = the diagonal tiles)
+  double* acc;  // accumulators [sets][9][n]
+};
+
+constexpr int kRotWarps = 4;
+constexpr int kRotThreads = 32 * kRotWarps;
+constexpr int kRotTile = 128 * kRotWarps;  // four targets per lane (two packed FP32x2 lanes)
+constexpr float kRotFar = 1e15f;           // position of the padding sources: g, f underflow
+
+constexpr size_t rot_smem_bytes() {
+  return size_t(kRotTile) * 9 * sizeof(double) +          // target-side FP64 carries
+         size_t(2) * kRotWarps * 32 * 9 * sizeof(float);  // source-side sums, double-buffered
+}
+
+struct RotSrc {
+  float x, y, z, s, ax, ay, az;
+};
+
+// Source j of the packed records (j < n), or a padding source far away with no strength.
+__device__ __forceinline__ RotSrc rot_load_src(const Rec<float2>* rec, int64_t j, int64_t n) {
+  if (j < n) {
+    const float4* p = reinterpret_cast<const float4*>(rec + j);
+    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+    return RotSrc{a.x, a.z, b.x, b.z, c.x, c.z, d.x};
+  }
+  return RotSrc{kRotFar, kRotFar, kRotFar, 1.f, 0.f, 0.f, 0.f};
+}
+
+template <class Op, bool DIAG>
+__global__ void __launch_bounds__(kRotThreads, 3)
+rot_sweep_kernel(const RotArgs a) {
+  constexpr int NV = Op::NV;
+  constexpr int T = kRotTile;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  double* car = reinterpret_cast<double*>(smem_raw);  // [NV][T]
+  float* jbuf = reinterpret_cast<float*>(smem_raw + size_t(T) * NV * sizeof(double));
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  int I, J, set_i, set_j;
+  if (DIAG) {
+    I = J = blockIdx.x;
+    set_i = 0;
+    set_j = 0;
+  } else {
+    const int q = blockIdx.x / a.nt, r = blockIdx.x - q * a.nt;
+    const int k = a.k0 + q, n1 = a.nt - k;
+    if (r < n1) {
+      I = r;
+      J = r + k;
+      set_i = 4 * q;
+      set_j = 4 * q + 1;
+    } else if (n1 > k) {
+      I = r - n1;
+      J = I + n1;
+      set_i = 4 * q + 2;
+      set_j = 4 * q + 3;
+    } else {
+      return;  // k == nt - k: the diagonal has only nt - k tile pairs
+    }
+  }
+  const int64_t i0 = int64_t(I) * T, j0 = int64_t(J) * T;
+  const int cnt = int((a.n - j0 < T) ? (a.n - j0) : T);
+
+  for (int q = tid; q < T * NV; q += kRotThreads) car[q] = 0.0;
+
+  // this lane's four targets: warp*128 + lane + {0, 32} (first packed lane) and + {64, 96}
+  int lt[4];
+  typename Op::OneSided::TgtT tg[2];
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    lt[2 * p] = warp * 128 + p * 64 + lane;
+    lt[2 * p + 1] = lt[2 * p] + 32;
+    const int64_t t0 = i0 + lt[2 * p], t1 = i0 + lt[2 * p + 1];
+    const Rec<float2>* recs[2] = {a.rec + (t0 < a.n ? t0 : a.n - 1),
+                                  a.rec + (t1 < a.n ? t1 : a.n - 1)};
+    tg[p] = make_tgt(recs);
+  }
+  float2 acc[2][NV];
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[p][v] = make_float2(0.f, 0.f);
+  __syncthreads();  // carries zeroed
+
+  const int nb = (cnt + 31) / 32;
+  RotSrc nxt = rot_load_src(a.rec, j0 + lane, j0 + cnt);
+  for (int b = 0; b < nb; ++b) {
+    RotSrc cur = nxt;  // the source this lane holds at step 0
+    if (b + 1 < nb) nxt = rot_load_src(a.rec, j0 + (b + 1) * 32 + lane, j0 + cnt);
+    float2 jv[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) jv[v] = make_float2(0.f, 0.f);
+    const int src_lane = (lane + 1) & 31;
+#pragma unroll 2
+    for (int step = 0; step < 32; ++step) {
+      const Src<float2> src{make_float2(cur.x, cur.x),   make_float2(cur.y, cur.y),
+                            make_float2(cur.z, cur.z),   make_float2(cur.s, cur.s),
+                            make_float2(cur.ax, cur.ax), make_float2(cur.ay, cur.ay),
+                            make_float2(cur.az, cur.az), make_float2(0.f, 0.f)};
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        if constexpr (DIAG)
+          Op::OneSided::pair(tg[p], acc[p], src, nullptr, 0);
+        else
+          Op::pair2(tg[p], acc[p], jv, src);
+      }
+      // pass the source (and its sums) one lane down: lane l now holds what lane l+1 held
+      cur.x = __shfl_sync(0xffffffffu, cur.x, src_lane);
+      cur.y = __shfl_sync(0xffffffffu, cur.y, src_lane);
+      cur.z = __shfl_sync(0xffffffffu, cur.z, src_lane);
+      cur.s = __shfl_sync(0xffffffffu, cur.s, src_lane);
+      cur.ax = __shfl_sync(0xffffffffu, cur.ax, src_lane);
+      cur.ay = __shfl_sync(0xffffffffu, cur.ay, src_lane);
+      cur.az = __shfl_sync(0xffffffffu, cur.az, src_lane);
+      if constexpr (!DIAG) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          jv[v].x = __shfl_sync(0xffffffffu, jv[v].x, src_lane);
+          jv[v].y = __shfl_sync(0xffffffffu, jv[v].y, src_lane);
+        }
+      }
+    }
+    // target side: this batch's FP32 sums into the FP64 carries (each thread its own rows)
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        car[v * T + lt[2 * p]] += double(acc[p][v].x);
+        car[v * T + lt[2 * p + 1]] += double(acc[p][v].y);
+        acc[p][v] = make_float2(0.f, 0.f);
+      }
+    }
+    if constexpr (!DIAG) {
+      // after 32 steps lane l holds the sums of source b*32 + l again
+      float* jb = jbuf + (b & 1) * (kRotWarps * 32 * NV);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) jb[(warp * 32 + lane) * NV + v] = jv[v].x + jv[v].y;
+      __syncthreads();  // one barrier per batch; jbuf is double-buffered
+      const int nsrc = (cnt - b * 32 < 32) ? cnt - b * 32 : 32;
+      for (int q = tid; q < nsrc * NV; q += kRotThreads) {
+        const int jj = q / NV, v = q - jj * NV;
+        double sum = 0.0;
+#pragma unroll
+        for (int w = 0; w < kRotWarps; ++w) sum += double(jb[(w * 32 + jj) * NV + v]);
+        a.acc[(int64_t(set_j) * NV + v) * a.n + (j0 + b * 32 + jj)] -= sum;
+      }
+    }
+  }
+  __syncthreads();
+  for (int q = tid; q < T * NV; q += kRotThreads) {
+    const int v = q / T, t = q - v * T;
+    if (i0 + t < a.n) a.acc[(int64_t(set_i) * NV + v) * a.n + (i0 + t)] += car[q];
+  }
+}
+
+}  // namespace vpm

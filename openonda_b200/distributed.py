@@ -80,7 +80,12 @@ class ShardedVelocityStretching:
         self.ws = torch.empty(max(self.ws_bytes, 256), dtype=torch.uint8, device=dev)
         self.u = torch.empty((self.m, 3), dtype=torch.float64, device=dev)
         self.g = torch.empty((self.m, 3), dtype=torch.float64, device=dev)
-        self.kernel_launches_per_call = 3  # pack, sweep, finalize
+        # pack, then the sweep's own launches (one-sided: sweep + finalize; both-sides sweep
+        # over all particles: zero, diagonal tiles, diagonal-pair launches, finalize)
+        self.sweep_launches = int(lib.vpm_sweep_launches(
+            _lib.OPS["velocity_and_strength_gradients"], self.pcode, self.m, self.n))
+        self.both_sides = self.sweep_launches > 2
+        self.kernel_launches_per_call = 1 + self.sweep_launches
 
     def pack(self, positions, strengths, radii):
         x = kernels._check_vec("positions", positions, self.m)

@@ -230,6 +230,12 @@ def total_enstrophy(positions, strengths, radii, ref_extra_4pi=True,
     return out
 
 
+def set_symmetric_min_n(n: int) -> int:
+    """Particle count from which the FP32-compensated fused velocity + stretching self sum
+    evaluates each unordered pair once for both particles; returns the previous value."""
+    return int(_lib.load().vpm_set_symmetric_min_n(int(n)))
+
+
 def device_errors(clear: bool = True) -> int:
     import ctypes
 

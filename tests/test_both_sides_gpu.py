@@ -1,0 +1,111 @@
+"""The both-sides sweep of the FP32-compensated fused velocity + stretching self sum
+(csrc/vpm_rot.cuh), forced on at small sizes so that two, three and many tiles, odd and even
+tile counts, several diagonal pairs per launch and a ragged last tile are covered: against
+the FP64 one-sided sweep (itself pinned to the reference), against the FP32 one-sided sweep,
+and bitwise repeatable."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import normwise
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture
+def both_sides_always():
+    from openonda_b200 import kernels
+
+    prev = kernels.set_symmetric_min_n(0)
+    yield
+    kernels.set_symmetric_min_n(prev)
+
+
+def _field(n, seed, ring=False):
+    from openonda_b200 import configs
+
+    if ring:
+        return configs.vortex_ring(16, n // 16, 1.0, 1.0, 0.1, nu=1e-3)
+    f = configs.random_cloud(n, seed=seed)
+    f.radii *= 4
+    return f
+
+
+def _dev32(f):
+    return [torch.from_numpy(np.asarray(z, np.float32).astype(np.float64)).cuda()
+            for z in (f.positions, f.strengths, f.radii)]
+
+
+@pytest.mark.parametrize("n,ring", [(1000, False), (1536, False), (3001, False), (2048, True),
+                                    (4096, True), (20000, False)])
+@pytest.mark.parametrize("uniform_core", [False, True])
+def test_both_sides_vs_fp64(n, ring, uniform_core):
+    from openonda_b200 import kernels
+
+    f = _field(n, 7 + n, ring)
+    if uniform_core:
+        f.radii[:] = f.radii[0]
+    x, a, s = _dev32(f)
+    prev = kernels.set_symmetric_min_n(1 << 40)
+    try:
+        one32 = kernels.velocity_and_strength_gradients(x, a, s, precision="fp32c",
+                                                        uniform_core=uniform_core)
+        ref = kernels.velocity_and_strength_gradients(x, a, s, precision="fp64")
+        kernels.set_symmetric_min_n(0)
+        plan = kernels.plan_info("velocity_and_strength_gradients", "fp32c", n, n)
+        assert plan["splits"] % 4 == 0 and plan["threads"] == 128  # the both-sides plan
+        both = kernels.velocity_and_strength_gradients(x, a, s, precision="fp32c",
+                                                       uniform_core=uniform_core)
+    finally:
+        kernels.set_symmetric_min_n(prev)
+    for k in range(2):
+        e_both = normwise(both[k].cpu().numpy(), ref[k].cpu().numpy())
+        e_one = normwise(one32[k].cpu().numpy(), ref[k].cpu().numpy())
+        print(f"n={n} ring={ring} uc={uniform_core} k={k}: both {e_both:.2e} one {e_one:.2e}")
+        # velocity: the FP32c bar; stretching: no worse than the one-sided FP32c sweep
+        # (on these coarse rings both exceed the ring-8192 figure)
+        assert e_both <= (1e-6 if k == 0 else max(5e-6, 1.5 * e_one)), (k, e_both, e_one)
+    assert kernels.device_errors() == 0
+
+
+def test_both_sides_is_deterministic(both_sides_always):
+    from openonda_b200 import kernels
+
+    x, a, s = _dev32(_field(5000, 3))
+    u1, g1 = kernels.velocity_and_strength_gradients(x, a, s, precision="fp32c")
+    u2, g2 = kernels.velocity_and_strength_gradients(x, a, s, precision="fp32c")
+    assert torch.equal(u1, u2) and torch.equal(g1, g2)
+
+
+def test_records_whole_set_and_shards(both_sides_always):
+    """vpm_sweep_records over all records (m = n) takes the both-sides sweep, target shards
+    (m < n) the one-sided one; both agree with the FP64 sweep."""
+    from openonda_b200 import _lib, kernels
+
+    n = 3000
+    f = _field(n, 11)
+    x, a, s = _dev32(f)
+    ref = kernels.velocity_and_strength_gradients(x, a, s, precision="fp64")
+    lib = _lib.load()
+    code = _lib.precision_code("fp32c")
+    rec = torch.empty(n * int(lib.vpm_record_bytes(code)), dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    _lib.check(lib.vpm_pack_records(x.data_ptr(), a.data_ptr(), s.data_ptr(), None, n, code,
+                                    rec.data_ptr(), st))
+    op = _lib.OPS["velocity_and_strength_gradients"]
+
+    def sweep(t0, m):
+        u = torch.empty((m, 3), dtype=torch.float64, device="cuda")
+        g = torch.empty((m, 3), dtype=torch.float64, device="cuda")
+        nb = kernels.workspace_bytes("velocity_and_strength_gradients", "fp32c", m, n)
+        ws = torch.empty(max(nb, 256), dtype=torch.uint8, device="cuda")
+        _lib.check(lib.vpm_sweep_records(op, rec.data_ptr(), n, t0, m, 0, u.data_ptr(),
+                                         g.data_ptr(), code, ws.data_ptr(), ws.numel(), st))
+        return u, g
+
+    full = sweep(0, n)
+    parts = [sweep(0, 1000), sweep(1000, 1200), sweep(2200, 800)]
+    for k, tol in ((0, 1e-6), (1, 5e-6)):
+        joined = torch.cat([p[k] for p in parts])
+        assert normwise(full[k].cpu().numpy(), ref[k].cpu().numpy()) <= tol
+        assert normwise(joined.cpu().numpy(), ref[k].cpu().numpy()) <= tol
