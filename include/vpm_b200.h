@@ -150,11 +150,12 @@ int vpm_velocity_and_strength_gradients(const double* positions, const double* s
                                         double* dalpha_dt, int precision, void* workspace,
                                         size_t workspace_bytes, void* stream);
 
-/* FP32-compensated self sums of velocity + stretching (vpm_velocity_and_strength_gradients,
- * and vpm_sweep_records over all records) with n >= this value evaluate each unordered pair
- * once for both particles (deterministic tile-pair schedule, about n / 1024 / m launches with
- * m diagonal pairs per launch).  Sets the threshold and returns the previous one (default
- * 131072).  No counterpart in the reference. */
+/* FP32-compensated self sums of velocity + stretching, velocity alone and PSE
+ * (vpm_velocity_and_strength_gradients, vpm_selfinduced_velocity,
+ * vpm_strength_gradients_pse, and vpm_sweep_records over all records) with n >= this value
+ * evaluate each unordered pair once for both particles (deterministic tile-pair schedule,
+ * about n / 1024 / m launches with m diagonal pairs per launch).  Sets the threshold and
+ * returns the previous one (default 65536).  No counterpart in the reference. */
 int64_t vpm_set_symmetric_min_n(int64_t n);
 /* Kernel launches of one sweep of `op` (sweep and finalize, not the packing of the inputs)
  * for m targets and n sources under the current plan; -1 on error. */

@@ -92,7 +92,7 @@ struct Plan {
 
 // FP32 self sums of velocity + stretching with at least this many particles evaluate each
 // unordered pair once for both particles (vpm_set_symmetric_min_n changes it).
-std::atomic<int64_t> g_sym_min_n{int64_t(1) << 17};
+std::atomic<int64_t> g_sym_min_n{int64_t(1) << 16};
 
 struct DevInfo {
   int sms = 0;
@@ -376,14 +376,23 @@ int zero_out(double* p, int64_t count, cudaStream_t st) {
   return VPM_OK;
 }
 
-// Both-sides sweep of the FP32 fused self sum (vpm_rot.cuh): launch 0 on the diagonal tiles,
-// then ceil(floor(nt/2) / m) launches of m diagonal pairs each.
+// Both-sides sweep of an FP32 self sum (vpm_rot.cuh): launch 0 on the diagonal tiles, then
+// ceil(floor(nt/2) / m) launches of m diagonal pairs each.
 template <class Op>
 struct RotSweep {
   static constexpr int NV = Op::NV;
   static constexpr int kMaxPairs = 8;
-  static constexpr size_t kSmem = rot_smem_bytes();
+  static constexpr size_t kSmem = rot_smem_bytes(NV);
   static int64_t tiles(int64_t n) { return (n + kRotTile - 1) / kRotTile; }
+  static size_t set_bytes(int64_t n) { return size_t(NV) * size_t(n) * sizeof(double); }
+
+  // Whether the planner takes this sweep for a self sum of n particles: the size threshold
+  // (vpm_set_symmetric_min_n), two tiles at least, and the 4 accumulator sets of one diagonal
+  // pair within the caller's partial-sum budget.
+  static bool usable(int64_t m, int64_t n, size_t max_partial_bytes) {
+    return m == n && n >= g_sym_min_n.load() && tiles(n) >= 2 &&
+           4 * set_bytes(n) <= max_partial_bytes;
+  }
 
   // Shared-memory attributes and resident CTAs per SM, once per device (cached like the
   // one-sided sweeps' plans).
@@ -412,7 +421,7 @@ struct RotSweep {
     return VPM_OK;
   }
 
-  static int plan(int64_t n, Plan* p) {
+  static int plan(int64_t n, Plan* p, size_t max_partial_bytes) {
     DevInfo d;
     int rc = device_info(&d);
     if (rc) return rc;
@@ -427,6 +436,7 @@ struct RotSweep {
     int best_m = 1;
     double best = -1.0;
     for (int m = 1; m <= kMaxPairs && m <= npairs; ++m) {
+      if (m > 1 && 4 * m * set_bytes(n) > max_partial_bytes) break;
       const double waves = double(m) * nt / slots;
       const double eff = waves / std::ceil(waves);
       if (eff > best + 1e-9) {
@@ -572,6 +582,8 @@ struct Ops {
   using VelStretch = OpVelStretch<T, REFINE, UC>;
   using LesStep = OpLesStep<T, REFINE, UC>;
   using VelStretchBoth = OpVelStretchBoth<REFINE, UC>;  // FP32 only
+  using VelBoth = OpVelBoth<REFINE, UC>;                // FP32 only
+  using PseBoth = OpPseBoth<REFINE, UC>;                // FP32 only
   using RhsVjp = OpRhsVjp<T, REFINE, false>;
   using RhsVjpPse = OpRhsVjp<T, REFINE, true>;
   using KeGrad = OpKeGrad<T, REFINE>;
@@ -584,6 +596,11 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
   using O = Ops<T, REFINE, UC>;
   switch (op) {
     case VPM_OP_SELFINDUCED_VELOCITY:
+      if constexpr (LaneTraits<T>::kLanes == 2) {
+        if (RotSweep<typename O::VelBoth>::usable(m, n, mpb))
+          return RotSweep<typename O::VelBoth>::plan(n, p, mpb);
+      }
+      return Sweep<typename O::Vel, T>::plan(m, n, p, mpb);
     case VPM_OP_TOTAL_HELICITY:
       return Sweep<typename O::Vel, T>::plan(m, n, p, mpb);
     case VPM_OP_INDUCED_VELOCITY_AT:
@@ -593,6 +610,10 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
     case VPM_OP_STRENGTH_GRADIENTS:
       return Sweep<typename O::Stretch, T>::plan(m, n, p, mpb);
     case VPM_OP_STRENGTH_GRADIENTS_PSE:
+      if constexpr (LaneTraits<T>::kLanes == 2) {
+        if (RotSweep<typename O::PseBoth>::usable(m, n, mpb))
+          return RotSweep<typename O::PseBoth>::plan(n, p, mpb);
+      }
       return Sweep<typename O::Pse, T>::plan(m, n, p, mpb);
     case VPM_OP_TOTAL_KINETIC_ENERGY:
       return Sweep<typename O::Ke, T>::plan(m, n, p, mpb);
@@ -600,9 +621,8 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
       return Sweep<typename O::Ens, T>::plan(m, n, p, mpb);
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
       if constexpr (LaneTraits<T>::kLanes == 2) {
-        if (m == n && n >= g_sym_min_n.load() &&
-            RotSweep<typename O::VelStretchBoth>::tiles(n) >= 2)
-          return RotSweep<typename O::VelStretchBoth>::plan(n, p);
+        if (RotSweep<typename O::VelStretchBoth>::usable(m, n, mpb))
+          return RotSweep<typename O::VelStretchBoth>::plan(n, p, mpb);
       }
       return Sweep<typename O::VelStretch, T>::plan(m, n, p, mpb);
     case VPM_OP_LES_STEP_SUMS:
@@ -719,7 +739,13 @@ int run(const Call& c) {
 
   switch (c.op) {
     case VPM_OP_SELFINDUCED_VELOCITY:
-      rc = Sweep<typename O::Vel, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+      rc = VPM_OK;
+      if constexpr (LaneTraits<T>::kLanes == 2) {
+        if (p.pairs)  // m == n: the targets are all the records (tgt_begin == 0)
+          rc = RotSweep<typename O::VelBoth>::launch(p, src, c.n, part, c.st);
+      }
+      if (!p.pairs)
+        rc = Sweep<typename O::Vel, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
       if (!rc) rc = finalize_vec<T, FIN_VEL, 3>(part, p.splits, c.m, tgt, c.out, nullptr, c.st);
       return rc;
     case VPM_OP_INDUCED_VELOCITY_AT:
@@ -736,7 +762,13 @@ int run(const Call& c) {
         rc = finalize_vec<T, FIN_STRETCH, 6>(part, p.splits, c.m, tgt, c.out, nullptr, c.st);
       return rc;
     case VPM_OP_STRENGTH_GRADIENTS_PSE:
-      rc = Sweep<typename O::Pse, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+      rc = VPM_OK;
+      if constexpr (LaneTraits<T>::kLanes == 2) {
+        if (p.pairs)
+          rc = RotSweep<typename O::PseBoth>::launch(p, src, c.n, part, c.st);
+      }
+      if (!p.pairs)
+        rc = Sweep<typename O::Pse, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
       if (!rc) rc = finalize_vec<T, FIN_PSE, 3>(part, p.splits, c.m, tgt, c.out, nullptr, c.st);
       return rc;
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:

@@ -1,10 +1,12 @@
-// vpm_rot.cuh -- both-sides sweep of the fused velocity + stretching self sum, FP32-
-// compensated, with the source side carried around the warp in registers.
+// vpm_rot.cuh -- both-sides sweeps of the FP32-compensated self sums (fused velocity +
+// stretching, velocity, PSE), with the source side carried around the warp in registers.
 //
-// The pair terms of (i <- j) and (j <- i) share r^2, the core, the rsqrt, g and f.  Seen from
-// particle j, with r = x_i - x_j as computed for target i:
-//   U_j += -g (r x a_i),   A_j += -g (a_j - a_i),   B_j += -h r,   h = f a_i . (r x a_j)
-// so one evaluation of an unordered pair costs 53 FP32 lane-ops instead of 2 x 38.
+// The pair terms of (i <- j) and (j <- i) share r^2, the core, the rsqrt and the kernel
+// values.  Seen from particle j, with r = x_i - x_j as computed for target i:
+//   U_j += -g (r x a_i),   A_j += -g (a_j - a_i),   B_j += -h r,   h = f a_i . (r x a_j),
+//   P_j += -k (a_j - a_i)   (PSE; nu_j is applied per particle in the finalize),
+// so one evaluation of an unordered pair costs 53 FP32 lane-ops instead of 2 x 38 for the
+// fused sum, 31 instead of 2 x 22 for the velocity and 24 instead of 2 x 21 for PSE.
 //
 // Warp layout: each lane holds four targets (two packed FP32x2 lanes) and one source of the
 // current batch of 32 (read from L2, the next batch prefetched).  In 32 steps every lane meets
@@ -12,16 +14,18 @@
 // move one lane down (__shfl_sync), so after the 32nd step each source is back in its lane
 // with its sums over the warp's 128 targets.  Warp shuffles are the second-scarcest resource
 // here (about one per two clocks per SM); four targets per lane keep them at 25 per 256
-// ordered pairs.  The source-side sums are then added over the CTA's warps in FP64 (fixed
-// order) and read-modify-written into the accumulator of the source particle.
+// ordered pairs for the fused sum.  The source-side sums are then added over the CTA's warps
+// in FP64 (fixed order) and added into the accumulator of the source particle with a
+// non-returning atomic.
 //
-// Tile-pair schedule (deterministic without atomics): particles form nt tiles of
-// T = 128 * WARPS.  A CTA owns one tile pair (I, J), I < J.  Diagonal pair q of a launch is
-// J - I = k (accumulator sets 4q / 4q+1 for the target / source side) together with
-// J - I = nt - k (sets 4q+2 / 4q+3): every (set, tile) is written by one CTA per launch, and
-// the launches run in stream order.  A launch runs m consecutive diagonal pairs (m chosen so
-// that its m * nt CTAs fill whole waves); launch 0 runs the diagonal tiles (I, I) one-sided
-// into set 0.  The finalize pass sums the 4m sets in order.
+// Tile-pair schedule: particles form nt tiles of T = 128 * WARPS.  A CTA owns one tile pair
+// (I, J), I < J.  Diagonal pair q of a launch is J - I = k (accumulator sets 4q / 4q+1 for
+// the target / source side) together with J - I = nt - k (sets 4q+2 / 4q+3): every
+// accumulator element has one writer per launch and the launches run in stream order, so the
+// atomic additions happen in a fixed order and the result is deterministic.  A launch runs m
+// consecutive diagonal pairs (m chosen so that its m * nt CTAs fill whole waves); launch 0
+// runs the diagonal tiles (I, I) one-sided into set 0.  The finalize pass sums the 4m sets in
+// order.
 //
 // Accumulation: target side in FP32 per batch of 32 sources, folded into FP64 carries held in
 // shared memory; source side in FP32 over the warp's 128 targets (each half of the packed
@@ -32,12 +36,29 @@
 
 namespace vpm {
 
+// Build parameters: warps per CTA, resident CTAs per SM the fused sum's registers are sized
+// for (VPM_ROT_MINB) and the three-sum operators' (VPM_ROT3_MINB), unroll of the 32 steps.
+#ifndef VPM_ROT_WARPS
+#define VPM_ROT_WARPS 4
+#endif
+#ifndef VPM_ROT_MINB
+#define VPM_ROT_MINB 3
+#endif
+#ifndef VPM_ROT3_MINB
+#define VPM_ROT3_MINB 3
+#endif
+#ifndef VPM_ROT_UNROLL
+#define VPM_ROT_UNROLL 8
+#endif
+
 // Fused velocity + stretching, both sides of the pair (FP32x2 lanes).
 template <bool REFINE, bool UC>
 struct OpVelStretchBoth {
   using V = float2;
   using OneSided = OpVelStretch<float2, REFINE, UC>;
   static constexpr int NV = 9;
+  static constexpr bool kSrcCore = !UC;  // the pair core needs the source's sigma
+  static constexpr int kMinBlocks = VPM_ROT_MINB;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -80,22 +101,89 @@ struct OpVelStretchBoth {
   }
 };
 
+// Self-induced velocity, both sides of the pair (FP32x2 lanes): U_j += -g (r x a_i).
+template <bool REFINE, bool UC>
+struct OpVelBoth {
+  using V = float2;
+  using OneSided = OpVel<float2, REFINE, UC>;
+  static constexpr int NV = 3;
+  static constexpr bool kSrcCore = !UC;
+  static constexpr int kMinBlocks = VPM_ROT3_MINB;
+  __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
+                                               const Src<V>& s) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    V sg, s2;
+    pair_core<UC>(t, s, sg, s2);
+    const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
+    const V y = rsqrt_lane<REFINE>(x);
+    const V y2 = y * y;
+    const V y5 = (y2 * y2) * y;
+    const V g = fma(splat<V>(1.5), s2, x) * y5;
+    const V cx = fma(ry, s.az, -(rz * s.ay));  // r x a_j
+    const V cy = fma(rz, s.ax, -(rx * s.az));
+    const V cz = fma(rx, s.ay, -(ry * s.ax));
+    acc[0] = fma(g, cx, acc[0]);
+    acc[1] = fma(g, cy, acc[1]);
+    acc[2] = fma(g, cz, acc[2]);
+    // source side, accumulated with the opposite sign (negated when it is stored)
+    const V ex = fma(ry, t.az, -(rz * t.ay));  // r x a_i
+    const V ey = fma(rz, t.ax, -(rx * t.az));
+    const V ez = fma(rx, t.ay, -(ry * t.ax));
+    jv[0] = fma(g, ex, jv[0]);
+    jv[1] = fma(g, ey, jv[1]);
+    jv[2] = fma(g, ez, jv[2]);
+  }
+};
+
+// PSE diffusion, both sides of the pair (FP32x2 lanes): the kernel value k is symmetric and
+// the exchange antisymmetric, P_j += -k (a_j - a_i); nu of each particle is applied by the
+// finalize.
+template <bool REFINE, bool UC>
+struct OpPseBoth {
+  using V = float2;
+  using OneSided = OpPse<float2, REFINE, UC>;
+  static constexpr int NV = 3;
+  static constexpr bool kSrcCore = !UC;
+  static constexpr int kMinBlocks = VPM_ROT3_MINB;
+  __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
+                                               const Src<V>& s) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    V sg, s2;
+    pair_core<UC>(t, s, sg, s2);
+    const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
+    const V y = rsqrt_lane<REFINE>(x);
+    const V z = sg * y;  // <= 1
+    const V z2 = z * z;
+    const V z4 = z2 * z2;
+    const V z7 = (z4 * z2) * z;
+    const V k = z7 * (y * y);
+    const V dx = s.ax - t.ax, dy = s.ay - t.ay, dz = s.az - t.az;
+    acc[0] = fma(k, dx, acc[0]);
+    acc[1] = fma(k, dy, acc[1]);
+    acc[2] = fma(k, dz, acc[2]);
+    jv[0] = fma(k, dx, jv[0]);  // negated when it is stored
+    jv[1] = fma(k, dy, jv[1]);
+    jv[2] = fma(k, dz, jv[2]);
+  }
+};
+
 struct RotArgs {
   const Rec<float2>* rec;  // packed records of all n particles
   int64_t n;
   int nt;       // tiles of kRotTile particles
   int k0;       // first diagonal of this launch (0 = the diagonal tiles)
-  double* acc;  // accumulators [sets][9][n]
+  double* acc;  // accumulators [sets][NV][n]
 };
 
-constexpr int kRotWarps = 4;
+constexpr int kRotWarps = VPM_ROT_WARPS;
+constexpr int kRotUnroll = VPM_ROT_UNROLL;
 constexpr int kRotThreads = 32 * kRotWarps;
 constexpr int kRotTile = 128 * kRotWarps;  // four targets per lane (two packed FP32x2 lanes)
 constexpr float kRotFar = 1e15f;           // position of the padding sources: g, f underflow
 
-constexpr size_t rot_smem_bytes() {
-  return size_t(kRotTile) * 9 * sizeof(double) +          // target-side FP64 carries
-         size_t(2) * kRotWarps * 32 * 9 * sizeof(float);  // source-side sums, double-buffered
+constexpr size_t rot_smem_bytes(int nv) {
+  return size_t(kRotTile) * nv * sizeof(double) +          // target-side FP64 carries
+         size_t(2) * kRotWarps * 32 * nv * sizeof(float);  // source-side sums, double-buffered
 }
 
 struct RotSrc {
@@ -113,7 +201,7 @@ __device__ __forceinline__ RotSrc rot_load_src(const Rec<float2>* rec, int64_t j
 }
 
 template <class Op, bool DIAG>
-__global__ void __launch_bounds__(kRotThreads, 3)
+__global__ void __launch_bounds__(kRotThreads, Op::kMinBlocks)
 rot_sweep_kernel(const RotArgs a) {
   constexpr int NV = Op::NV;
   constexpr int T = kRotTile;
@@ -177,7 +265,7 @@ rot_sweep_kernel(const RotArgs a) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) jv[v] = make_float2(0.f, 0.f);
     const int src_lane = (lane + 1) & 31;
-#pragma unroll 2
+#pragma unroll kRotUnroll
     for (int step = 0; step < 32; ++step) {
       const Src<float2> src{make_float2(cur.x, cur.x),   make_float2(cur.y, cur.y),
                             make_float2(cur.z, cur.z),   make_float2(cur.s, cur.s),
@@ -194,7 +282,7 @@ rot_sweep_kernel(const RotArgs a) {
       cur.x = __shfl_sync(0xffffffffu, cur.x, src_lane);
       cur.y = __shfl_sync(0xffffffffu, cur.y, src_lane);
       cur.z = __shfl_sync(0xffffffffu, cur.z, src_lane);
-      cur.s = __shfl_sync(0xffffffffu, cur.s, src_lane);
+      if constexpr (Op::kSrcCore) cur.s = __shfl_sync(0xffffffffu, cur.s, src_lane);
       cur.ax = __shfl_sync(0xffffffffu, cur.ax, src_lane);
       cur.ay = __shfl_sync(0xffffffffu, cur.ay, src_lane);
       cur.az = __shfl_sync(0xffffffffu, cur.az, src_lane);
@@ -228,14 +316,16 @@ rot_sweep_kernel(const RotArgs a) {
         double sum = 0.0;
 #pragma unroll
         for (int w = 0; w < kRotWarps; ++w) sum += double(jb[(w * 32 + jj) * NV + v]);
-        a.acc[(int64_t(set_j) * NV + v) * a.n + (j0 + b * 32 + jj)] -= sum;
+        // the only writer of this element in this launch, so the fire-and-forget reduction
+        // adds in a fixed order (launch order) and the thread does not wait for the load
+        atomicAdd(&a.acc[(int64_t(set_j) * NV + v) * a.n + (j0 + b * 32 + jj)], -sum);
       }
     }
   }
   __syncthreads();
   for (int q = tid; q < T * NV; q += kRotThreads) {
     const int v = q / T, t = q - v * T;
-    if (i0 + t < a.n) a.acc[(int64_t(set_i) * NV + v) * a.n + (i0 + t)] += car[q];
+    if (i0 + t < a.n) atomicAdd(&a.acc[(int64_t(set_i) * NV + v) * a.n + (i0 + t)], car[q]);
   }
 }
 

@@ -231,9 +231,20 @@ def total_enstrophy(positions, strengths, radii, ref_extra_4pi=True,
 
 
 def set_symmetric_min_n(n: int) -> int:
-    """Particle count from which the FP32-compensated fused velocity + stretching self sum
-    evaluates each unordered pair once for both particles; returns the previous value."""
+    """Particle count from which the FP32-compensated self sums of velocity + stretching,
+    velocity and PSE evaluate each unordered pair once for both particles; returns the
+    previous value."""
     return int(_lib.load().vpm_set_symmetric_min_n(int(n)))
+
+
+def sweep_launches(op: str, precision: str, m: int, n: int, uniform_core: bool = False) -> int:
+    """Kernel launches of one sweep of ``op`` (sweep and finalize) under the current plan."""
+    v = int(_lib.load().vpm_sweep_launches(_lib.OPS[op],
+                                           _lib.precision_code(precision, uniform_core),
+                                           int(m), int(n)))
+    if v < 0:
+        raise _lib.VPMError(_lib.VPM_ERR_ARG, f"no plan for {op} at m={m}, n={n}")
+    return v
 
 
 def device_errors(clear: bool = True) -> int:

@@ -1,5 +1,5 @@
-"""The both-sides sweep of the FP32-compensated fused velocity + stretching self sum
-(csrc/vpm_rot.cuh), forced on at small sizes so that two, three and many tiles, odd and even
+"""The both-sides sweeps of the FP32-compensated self sums (fused velocity + stretching,
+velocity, PSE; csrc/vpm_rot.cuh), forced on at small sizes so that two, three and many tiles, odd and even
 tile counts, several diagonal pairs per launch and a ragged last tile are covered: against
 the FP64 one-sided sweep (itself pinned to the reference), against the FP32 one-sided sweep,
 and bitwise repeatable."""
@@ -109,3 +109,50 @@ def test_records_whole_set_and_shards(both_sides_always):
         joined = torch.cat([p[k] for p in parts])
         assert normwise(full[k].cpu().numpy(), ref[k].cpu().numpy()) <= tol
         assert normwise(joined.cpu().numpy(), ref[k].cpu().numpy()) <= tol
+
+
+@pytest.mark.parametrize("n,ring", [(1000, False), (1536, False), (3001, False), (2048, True),
+                                    (4096, True), (20000, False)])
+@pytest.mark.parametrize("uniform_core", [False, True])
+@pytest.mark.parametrize("op", ["selfinduced_velocity", "strength_gradients_pse"])
+def test_velocity_and_pse_both_sides_vs_fp64(op, n, ring, uniform_core):
+    """The velocity and PSE sums take the same both-sides schedule: FP32c bar against the
+    FP64 one-sided sweep, and no worse than the one-sided FP32c sweep."""
+    from openonda_b200 import kernels
+
+    f = _field(n, 5 + n, ring)
+    if uniform_core:
+        f.radii[:] = f.radii[0]
+    x, a, s = _dev32(f)
+    nu = torch.from_numpy(np.ascontiguousarray(f.viscosities)).cuda()
+    fn = getattr(kernels, op)
+    args = (x, a, s) if op == "selfinduced_velocity" else (x, a, s, nu)
+    prev = kernels.set_symmetric_min_n(1 << 40)
+    try:
+        one32 = fn(*args, precision="fp32c", uniform_core=uniform_core)
+        ref = fn(*args, precision="fp64")
+        kernels.set_symmetric_min_n(0)
+        plan = kernels.plan_info(op, "fp32c", n, n)
+        assert plan["splits"] % 4 == 0 and plan["threads"] == 128  # the both-sides plan
+        both = fn(*args, precision="fp32c", uniform_core=uniform_core)
+        again = fn(*args, precision="fp32c", uniform_core=uniform_core)
+    finally:
+        kernels.set_symmetric_min_n(prev)
+    e_both = normwise(both.cpu().numpy(), ref.cpu().numpy())
+    e_one = normwise(one32.cpu().numpy(), ref.cpu().numpy())
+    print(f"{op} n={n} ring={ring} uc={uniform_core}: both {e_both:.2e} one {e_one:.2e}")
+    assert e_both <= 1e-6, (e_both, e_one)
+    assert torch.equal(both, again)
+    assert kernels.device_errors() == 0
+
+
+def test_helicity_and_shards_stay_one_sided(both_sides_always):
+    """Only whole-set self sums of the FP32c precisions take the both-sides sweep."""
+    from openonda_b200 import kernels
+
+    n = 4096
+    assert kernels.plan_info("selfinduced_velocity", "fp32c", n, n)["splits"] % 4 == 0
+    assert kernels.sweep_launches("total_helicity", "fp32c", n, n) == 2
+    assert kernels.sweep_launches("selfinduced_velocity", "fp32c", 1000, n) == 2
+    assert kernels.sweep_launches("strength_gradients_pse", "fp64", n, n) == 2
+    assert kernels.sweep_launches("strength_gradients_pse", "fp32c", n, n) > 3
