@@ -584,6 +584,7 @@ struct Ops {
   using VelStretchBoth = OpVelStretchBoth<REFINE, UC>;  // FP32 only
   using VelBoth = OpVelBoth<REFINE, UC>;                // FP32 only
   using PseBoth = OpPseBoth<REFINE, UC>;                // FP32 only
+  using LesStepBoth = OpLesStepBoth<REFINE, UC>;        // FP32 only
   using RhsVjp = OpRhsVjp<T, REFINE, false>;
   using RhsVjpPse = OpRhsVjp<T, REFINE, true>;
   using KeGrad = OpKeGrad<T, REFINE>;
@@ -626,6 +627,10 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
       }
       return Sweep<typename O::VelStretch, T>::plan(m, n, p, mpb);
     case VPM_OP_LES_STEP_SUMS:
+      if constexpr (LaneTraits<T>::kLanes == 2) {
+        if (RotSweep<typename O::LesStepBoth>::usable(m, n, mpb))
+          return RotSweep<typename O::LesStepBoth>::plan(n, p, mpb);
+      }
       return Sweep<typename O::LesStep, T>::plan(m, n, p, mpb);
     case VPM_OP_RHS_VJP:
       return Sweep<typename O::RhsVjp, T>::plan(m, n, p, mpb);
@@ -788,7 +793,12 @@ int run(const Call& c) {
       return rc;
     case VPM_OP_LES_STEP_SUMS: {
       using Op = typename O::LesStep;
-      rc = Sweep<Op, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
+      rc = VPM_OK;
+      if constexpr (LaneTraits<T>::kLanes == 2) {
+        if (p.pairs)
+          rc = RotSweep<typename O::LesStepBoth>::launch(p, src, c.n, part, c.st);
+      }
+      if (!p.pairs) rc = Sweep<Op, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
       if (!rc)
         rc = finalize_vec<T, FIN_LES, Op::NV>(part, p.splits, c.m, tgt, c.out, c.out2, c.st,
                                                c.out3);

@@ -1,12 +1,14 @@
 // vpm_rot.cuh -- both-sides sweeps of the FP32-compensated self sums (fused velocity +
-// stretching, velocity, PSE), with the source side carried around the warp in registers.
+// stretching, velocity, PSE, the LES step sums), with the source side carried around the warp
+// in registers.
 //
 // The pair terms of (i <- j) and (j <- i) share r^2, the core, the rsqrt and the kernel
 // values.  Seen from particle j, with r = x_i - x_j as computed for target i:
 //   U_j += -g (r x a_i),   A_j += -g (a_j - a_i),   B_j += -h r,   h = f a_i . (r x a_j),
 //   P_j += -k (a_j - a_i)   (PSE; nu_j is applied per particle in the finalize),
 // so one evaluation of an unordered pair costs 53 FP32 lane-ops instead of 2 x 38 for the
-// fused sum, 31 instead of 2 x 22 for the velocity and 24 instead of 2 x 21 for PSE.
+// fused sum, 31 instead of 2 x 22 for the velocity, 24 instead of 2 x 21 for PSE and 69-82
+// instead of 2 x 52-56 for the four LES step sums.
 //
 // Warp layout: each lane holds four targets (two packed FP32x2 lanes) and one source of the
 // current batch of 32 (read from L2, the next batch prefetched).  In 32 steps every lane meets
@@ -36,8 +38,9 @@
 
 namespace vpm {
 
-// Build parameters: warps per CTA, resident CTAs per SM the fused sum's registers are sized
-// for (VPM_ROT_MINB) and the three-sum operators' (VPM_ROT3_MINB), unroll of the 32 steps.
+// Build parameters: warps per CTA, resident CTAs per SM the registers are sized for (fused
+// sum VPM_ROT_MINB, three-sum operators VPM_ROT3_MINB, LES step VPM_ROT15_MINB: its 77 KB of
+// shared memory allow two), unroll of the 32 steps.
 #ifndef VPM_ROT_WARPS
 #define VPM_ROT_WARPS 4
 #endif
@@ -47,8 +50,14 @@ namespace vpm {
 #ifndef VPM_ROT3_MINB
 #define VPM_ROT3_MINB 3
 #endif
+#ifndef VPM_ROT15_MINB
+#define VPM_ROT15_MINB 2
+#endif
 #ifndef VPM_ROT_UNROLL
 #define VPM_ROT_UNROLL 8
+#endif
+#ifndef VPM_ROT15_UNROLL
+#define VPM_ROT15_UNROLL 2
 #endif
 
 // Fused velocity + stretching, both sides of the pair (FP32x2 lanes).
@@ -59,6 +68,7 @@ struct OpVelStretchBoth {
   static constexpr int NV = 9;
   static constexpr bool kSrcCore = !UC;  // the pair core needs the source's sigma
   static constexpr int kMinBlocks = VPM_ROT_MINB;
+  static constexpr int kUnroll = VPM_ROT_UNROLL;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -109,6 +119,7 @@ struct OpVelBoth {
   static constexpr int NV = 3;
   static constexpr bool kSrcCore = !UC;
   static constexpr int kMinBlocks = VPM_ROT3_MINB;
+  static constexpr int kUnroll = VPM_ROT_UNROLL;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -145,6 +156,7 @@ struct OpPseBoth {
   static constexpr int NV = 3;
   static constexpr bool kSrcCore = !UC;
   static constexpr int kMinBlocks = VPM_ROT3_MINB;
+  static constexpr int kUnroll = VPM_ROT_UNROLL;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -167,6 +179,100 @@ struct OpPseBoth {
   }
 };
 
+// The four sums of a dynamic-LES step (OpLesStep), both sides of the pair (FP32x2 lanes):
+// velocity and stretching as OpVelStretchBoth; the vorticity filter sum uses the core of the
+// particle that is summed over, so target i takes s_j^4 (r^2 + s_j^2)^-7/2 a_j and particle
+// j takes s_i^4 (r^2 + s_i^2)^-7/2 a_i (one rsqrt each; with uniform cores both equal the
+// pair core's y and need none); the enstrophy filter sum (x + 2.2 s^2) y^3 is symmetric.
+// Vorticity and enstrophy are symmetric sums, so their source-side terms enter negated (the
+// stored value is negated once more).  Pairs with r^2 <= 1e-8 add no vorticity.  69 FP32
+// lane-ops per unordered pair with uniform cores, about 82 without (one-sided: 2 x 52,
+// 2 x 56).  255 registers per thread: two CTAs per SM, step loop unrolled 2.
+template <bool REFINE, bool UC>
+struct OpLesStepBoth {
+  using V = float2;
+  using OneSided = OpLesStep<float2, REFINE, UC>;
+  static constexpr int NV = 15;
+  static constexpr bool kSrcCore = !UC;
+  static constexpr int kMinBlocks = VPM_ROT15_MINB;
+  static constexpr int kUnroll = VPM_ROT15_UNROLL;
+  __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
+                                               const Src<V>& s) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    V sg, s2;
+    pair_core<UC>(t, s, sg, s2);
+    const V r2 = fma(rx, rx, fma(ry, ry, rz * rz));
+    const V x = r2 + s2;
+    const V y = rsqrt_lane<REFINE>(x);
+    const V y2 = y * y;
+    const V y3 = y2 * y;
+    const V y5 = y3 * y2;
+    const V t1 = fma(splat<V>(1.5), s2, x);
+    const V g = t1 * y5;
+    const V f = (t1 + s2) * (y5 * y2);
+    const V cx = fma(ry, s.az, -(rz * s.ay));  // r x a_j
+    const V cy = fma(rz, s.ax, -(rx * s.az));
+    const V cz = fma(rx, s.ay, -(ry * s.ax));
+    acc[0] = fma(g, cx, acc[0]);
+    acc[1] = fma(g, cy, acc[1]);
+    acc[2] = fma(g, cz, acc[2]);
+    const V dx = s.ax - t.ax, dy = s.ay - t.ay, dz = s.az - t.az;
+    acc[3] = fma(g, dx, acc[3]);
+    acc[4] = fma(g, dy, acc[4]);
+    acc[5] = fma(g, dz, acc[5]);
+    const V h = f * fma(t.ax, cx, fma(t.ay, cy, t.az * cz));
+    acc[6] = fma(h, rx, acc[6]);
+    acc[7] = fma(h, ry, acc[7]);
+    acc[8] = fma(h, rz, acc[8]);
+    const V ex = fma(ry, t.az, -(rz * t.ay));  // r x a_i
+    const V ey = fma(rz, t.ax, -(rx * t.az));
+    const V ez = fma(rx, t.ay, -(ry * t.ax));
+    jv[0] = fma(g, ex, jv[0]);
+    jv[1] = fma(g, ey, jv[1]);
+    jv[2] = fma(g, ez, jv[2]);
+    jv[3] = fma(g, dx, jv[3]);
+    jv[4] = fma(g, dy, jv[4]);
+    jv[5] = fma(g, dz, jv[5]);
+    jv[6] = fma(h, rx, jv[6]);
+    jv[7] = fma(h, ry, jv[7]);
+    jv[8] = fma(h, rz, jv[8]);
+    // vorticity filter sums: kernel values zeroed for r^2 <= 1e-8
+    const float eps = float(kRefEps);
+    V ki, kj;
+    if constexpr (UC) {
+      const V y7 = (y3 * y3) * y;
+      ki = t.s4c * y7;
+      kj = ki;
+    } else {
+      const V sj2 = s.s * s.s;
+      const V yi = rsqrt_lane<REFINE>(r2 + sj2);  // source core: target i's sum
+      const V yi2 = yi * yi;
+      const V yi3 = yi2 * yi;
+      ki = (sj2 * sj2) * ((yi3 * yi3) * yi);
+      const V yj = rsqrt_lane<REFINE>(r2 + t.s2c);  // target core: particle j's sum
+      const V yj2 = yj * yj;
+      const V yj3 = yj2 * yj;
+      kj = t.s4c * ((yj3 * yj3) * yj);
+    }
+    ki = make_float2(r2.x > eps ? ki.x : 0.f, r2.y > eps ? ki.y : 0.f);
+    kj = make_float2(r2.x > eps ? kj.x : 0.f, r2.y > eps ? kj.y : 0.f);
+    acc[9] = fma(ki, s.ax, acc[9]);
+    acc[10] = fma(ki, s.ay, acc[10]);
+    acc[11] = fma(ki, s.az, acc[11]);
+    jv[9] = fma(-kj, t.ax, jv[9]);
+    jv[10] = fma(-kj, t.ay, jv[10]);
+    jv[11] = fma(-kj, t.az, jv[11]);
+    // enstrophy filter sum (pair core)
+    const V ke = fma(splat<V>(2.2), s2, x) * y3;
+    acc[12] = fma(ke, s.ax, acc[12]);
+    acc[13] = fma(ke, s.ay, acc[13]);
+    acc[14] = fma(ke, s.az, acc[14]);
+    jv[12] = fma(-ke, t.ax, jv[12]);
+    jv[13] = fma(-ke, t.ay, jv[13]);
+    jv[14] = fma(-ke, t.az, jv[14]);
+  }
+};
+
 struct RotArgs {
   const Rec<float2>* rec;  // packed records of all n particles
   int64_t n;
@@ -176,7 +282,6 @@ struct RotArgs {
 };
 
 constexpr int kRotWarps = VPM_ROT_WARPS;
-constexpr int kRotUnroll = VPM_ROT_UNROLL;
 constexpr int kRotThreads = 32 * kRotWarps;
 constexpr int kRotTile = 128 * kRotWarps;  // four targets per lane (two packed FP32x2 lanes)
 constexpr float kRotFar = 1e15f;           // position of the padding sources: g, f underflow
@@ -265,7 +370,7 @@ rot_sweep_kernel(const RotArgs a) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) jv[v] = make_float2(0.f, 0.f);
     const int src_lane = (lane + 1) & 31;
-#pragma unroll kRotUnroll
+#pragma unroll Op::kUnroll
     for (int step = 0; step < 32; ++step) {
       const Src<float2> src{make_float2(cur.x, cur.x),   make_float2(cur.y, cur.y),
                             make_float2(cur.z, cur.z),   make_float2(cur.s, cur.s),

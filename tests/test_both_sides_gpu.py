@@ -1,5 +1,5 @@
 """The both-sides sweeps of the FP32-compensated self sums (fused velocity + stretching,
-velocity, PSE; csrc/vpm_rot.cuh), forced on at small sizes so that two, three and many tiles, odd and even
+velocity, PSE, the LES step sums; csrc/vpm_rot.cuh), forced on at small sizes so that two, three and many tiles, odd and even
 tile counts, several diagonal pairs per launch and a ragged last tile are covered: against
 the FP64 one-sided sweep (itself pinned to the reference), against the FP32 one-sided sweep,
 and bitwise repeatable."""
@@ -156,3 +156,41 @@ def test_helicity_and_shards_stay_one_sided(both_sides_always):
     assert kernels.sweep_launches("selfinduced_velocity", "fp32c", 1000, n) == 2
     assert kernels.sweep_launches("strength_gradients_pse", "fp64", n, n) == 2
     assert kernels.sweep_launches("strength_gradients_pse", "fp32c", n, n) > 3
+
+
+@pytest.mark.parametrize("n,ring", [(1000, False), (3001, False), (2048, True), (4096, True),
+                                    (20000, False)])
+@pytest.mark.parametrize("uniform_core", [False, True])
+def test_les_step_sums_both_sides_vs_fp64(n, ring, uniform_core):
+    """The four LES step sums (velocity, stretching, particle vorticity with the source core,
+    enstrophy filter sum) on the both-sides schedule against the FP64 one-sided sweep, and
+    no worse than the one-sided FP32c sweep; coincident particles add no vorticity."""
+    from openonda_b200 import kernels
+
+    f = _field(n, 9 + n, ring)
+    if uniform_core:
+        f.radii[:] = f.radii[0]
+    if not ring:
+        f.positions[7] = f.positions[n - 3]  # coincident pair in different tiles
+    x, a, s = _dev32(f)
+    prev = kernels.set_symmetric_min_n(1 << 40)
+    try:
+        one32 = kernels.les_step_sums(x, a, s, precision="fp32c", uniform_core=uniform_core)
+        ref = kernels.les_step_sums(x, a, s, precision="fp64")
+        kernels.set_symmetric_min_n(0)
+        plan = kernels.plan_info("les_step_sums", "fp32c", n, n)
+        assert plan["splits"] % 4 == 0 and plan["threads"] == 128  # the both-sides plan
+        both = kernels.les_step_sums(x, a, s, precision="fp32c", uniform_core=uniform_core)
+        again = kernels.les_step_sums(x, a, s, precision="fp32c", uniform_core=uniform_core)
+    finally:
+        kernels.set_symmetric_min_n(prev)
+    for k in range(3):
+        e_both = normwise(both[k].cpu().numpy(), ref[k].cpu().numpy())
+        e_one = normwise(one32[k].cpu().numpy(), ref[k].cpu().numpy())
+        print(f"les n={n} ring={ring} uc={uniform_core} k={k}: both {e_both:.2e} "
+              f"one {e_one:.2e}")
+        assert e_both <= (1e-6 if k != 1 else max(5e-6, 1.5 * e_one)), (k, e_both, e_one)
+        assert torch.equal(both[k], again[k])
+    e_ref, e_got = float(ref[3]), float(both[3])
+    assert abs(e_got - e_ref) <= 1e-6 * abs(e_ref)
+    assert kernels.device_errors() == 0
