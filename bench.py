@@ -389,6 +389,46 @@ def main():
                             "structure restated in CUDA C++)"}
         del xa, aa, sa, outn
 
+    # ---- adjoint: one VJP sweep of the right-hand side (u, S [+ P]) against one forward
+    # evaluation of it, N = 65536 random cloud, cotangents N(0,1) ----
+    adjoint = None
+    if world == 1:
+        from openonda_b200 import autodiff
+
+        na = min(n, 65536)
+        xa = torch.from_numpy(x_h[:na]).to(dev)
+        aa = torch.from_numpy(a_h[:na]).to(dev)
+        sa = torch.from_numpy(s_h[:na]).to(dev)
+        nua = torch.full((na,), 1e-4, dtype=torch.float64, device=dev)
+        gen = torch.Generator().manual_seed(1)
+        gu = torch.randn((na, 3), generator=gen, dtype=torch.float64).to(dev)
+        gr = torch.randn((na, 3), generator=gen, dtype=torch.float64).to(dev)
+        adjoint = {"n": na, "steps": 3}
+        grads = {}
+        for prec in ("fp32c", "fp64"):
+            def fwd():
+                return kernels.velocity_and_strength_gradients(xa, aa, sa, precision=prec)
+
+            def fwd_pse():
+                return (fwd(), kernels.strength_gradients_pse(xa, aa, sa, nua, precision=prec))
+
+            tf, _, _ = timed(fwd, 3, 1)
+            tb, grads[prec], _ = timed(
+                lambda: autodiff.rhs_vjp(xa, aa, sa, None, gu, gr, precision=prec), 3, 1)
+            tfp, _, _ = timed(fwd_pse, 3, 1)
+            tbp, _, _ = timed(
+                lambda: autodiff.rhs_vjp(xa, aa, sa, nua, gu, gr, precision=prec), 3, 1)
+            adjoint[prec] = {"forward_ms": round(tf / 3 * 1e3, 3),
+                             "vjp_ms": round(tb / 3 * 1e3, 3),
+                             "vjp_over_forward": round(tb / tf, 3),
+                             "forward_pse_ms": round(tfp / 3 * 1e3, 3),
+                             "vjp_pse_ms": round(tbp / 3 * 1e3, 3),
+                             "vjp_pse_over_forward_pse": round(tbp / tfp, 3)}
+        adjoint["grad_rel_err_fp32c_vs_fp64"] = {
+            k: normwise(grads["fp32c"][i], grads["fp64"][i])
+            for i, k in enumerate(("positions", "strengths", "radii"))}
+        del xa, aa, sa, nua, gu, gr, grads
+
     # ---- end to end through the public API, host buffers (pinned), copies timed ----
     xp = torch.from_numpy(x_h[start:stop]).pin_memory()
     ap_ = torch.from_numpy(a_h[start:stop]).pin_memory()
@@ -461,6 +501,7 @@ def main():
             "reference_algorithm_gpu": naive,
             "speedup_vs_reference_algorithm_gpu":
                 None if naive is None else round(value / naive["gpairs_s"], 1),
+            "adjoint": adjoint,
             "roofline": {"bound": "fp32", "achieved": round(achieved, 3),
                          "peak": round(peak, 3), "unit": "TFLOP/s",
                          "frac": round(achieved / peak, 4), "traffic": tr,

@@ -246,17 +246,39 @@ GRAPH_CASES["ring_dns_pse_rk4_uniform_core"] = dict(
 GRAPH_CASES["ring_dns_cs_rk2_uniform_core"] = dict(
     flow_model="DNS", viscous_scheme="CoreSpreading", time_integration_method="RK2",
     time_step_size=0.005, field="ring")
+# FP32c self sums on the both-sides schedule (forced on below its size threshold)
+GRAPH_CASES["les_pse_rk4_fp32c_both_sides"] = dict(
+    flow_model="LES", viscous_scheme="PSE", time_integration_method="RK4",
+    time_step_size=0.005, precision="fp32c", both_sides=True)
+GRAPH_CASES["ring_dns_pse_rk4_fp32c_both_sides"] = dict(
+    flow_model="DNS", viscous_scheme="PSE", time_integration_method="RK4",
+    time_step_size=0.005, precision="fp32c", field="ring", both_sides=True)
 
 
 @pytest.mark.parametrize("name", sorted(GRAPH_CASES))
 def test_advance_with_cuda_graph_equals_eager_loop(tmp_path, name):
     """advance() replays one captured step from time step 3 on; it must reproduce the
     reference loop (update_velocities, update_strengths, update_state) bit for bit,
-    including the steps where a backup is due and after a change that forces a recapture."""
-    import torch
+    including the steps where a backup is due and after a change that forces a recapture.
+    The FP32c cases run with the both-sides schedule forced on (its zeroing, diagonal and
+    diagonal-pair launches inside the captured graph); the others with it off."""
+    from openonda_b200 import kernels
 
     cfg = dict(GRAPH_CASES[name])
     f = _field(cfg.pop("field", "cloud"))
+    both_sides = cfg.pop("both_sides", False)
+    prev = kernels.set_symmetric_min_n(0 if both_sides else 1 << 40)
+    try:
+        if both_sides:
+            assert kernels.sweep_launches("selfinduced_velocity", "fp32c", f.n, f.n) > 3
+        _advance_vs_eager(tmp_path, name, cfg, f)
+    finally:
+        kernels.set_symmetric_min_n(prev)
+
+
+def _advance_vs_eager(tmp_path, name, cfg, f):
+    import torch
+
     from openonda_b200.vpm.vpmModule import ParticleSystem
 
     def make(sub):
