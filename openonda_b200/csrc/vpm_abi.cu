@@ -382,8 +382,9 @@ template <class Op>
 struct RotSweep {
   static constexpr int NV = Op::NV;
   static constexpr int kMaxPairs = 8;
-  static constexpr size_t kSmem = rot_smem_bytes(NV);
-  static int64_t tiles(int64_t n) { return (n + kRotTile - 1) / kRotTile; }
+  static constexpr int kTile = rot_tile<Op>();
+  static constexpr size_t kSmem = rot_smem_bytes(NV, kTile);
+  static int64_t tiles(int64_t n) { return (n + kTile - 1) / kTile; }
   static size_t set_bytes(int64_t n) { return size_t(NV) * size_t(n) * sizeof(double); }
 
   // Whether the planner takes this sweep for a self sum of n particles: the size threshold
@@ -451,13 +452,13 @@ struct RotSweep {
     p->chunk = n;
     p->smem = kSmem;
     p->threads = kRotThreads;
-    p->r = 4;
+    p->r = 2 * Op::kP;
     p->nv = NV;
     return VPM_OK;
   }
 
   // acc: [4 * pairs][NV][n] FP64, zeroed here.
-  static int launch(const Plan& p, const Rec<float2>* rec, int64_t n, double* acc,
+  static int launch(const Plan& p, const void* rec, int64_t n, double* acc,
                     cudaStream_t st) {
     const int nt = int(tiles(n));
     int occ = 1;
@@ -585,6 +586,7 @@ struct Ops {
   using VelBoth = OpVelBoth<REFINE, UC>;                // FP32 only
   using PseBoth = OpPseBoth<REFINE, UC>;                // FP32 only
   using LesStepBoth = OpLesStepBoth<REFINE, UC>;        // FP32 only
+  using RhsVjpBoth = OpRhsVjpBoth<REFINE>;              // FP32 only
   using RhsVjp = OpRhsVjp<T, REFINE, false>;
   using RhsVjpPse = OpRhsVjp<T, REFINE, true>;
   using KeGrad = OpKeGrad<T, REFINE>;
@@ -633,6 +635,10 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
       }
       return Sweep<typename O::LesStep, T>::plan(m, n, p, mpb);
     case VPM_OP_RHS_VJP:
+      if constexpr (LaneTraits<T>::kLanes == 2) {
+        if (RotSweep<typename O::RhsVjpBoth>::usable(m, n, mpb))
+          return RotSweep<typename O::RhsVjpBoth>::plan(n, p, mpb);
+      }
       return Sweep<typename O::RhsVjp, T>::plan(m, n, p, mpb);
     case VPM_OP_RHS_VJP_PSE:
       return Sweep<typename O::RhsVjpPse, T>::plan(m, n, p, mpb);
@@ -935,7 +941,11 @@ int run_grad(const GradCall& c) {
     finalize_vjp_kernel<T, O::RhsVjpPse::NV, true>
         <<<blocks, 256, 0, c.st>>>(part, p.splits, c.n, rec, c.ox, c.oa, c.os, c.onu);
   } else {
-    rc = Sweep<typename O::RhsVjp, T>::launch(p, rec, c.n, 0, rec, c.n, part, c.st);
+    rc = VPM_OK;
+    if constexpr (LaneTraits<T>::kLanes == 2) {
+      if (p.pairs) rc = RotSweep<typename O::RhsVjpBoth>::launch(p, rec, c.n, part, c.st);
+    }
+    if (!p.pairs) rc = Sweep<typename O::RhsVjp, T>::launch(p, rec, c.n, 0, rec, c.n, part, c.st);
     if (rc) return rc;
     finalize_vjp_kernel<T, O::RhsVjp::NV, false>
         <<<blocks, 256, 0, c.st>>>(part, p.splits, c.n, rec, c.ox, c.oa, c.os, c.onu);

@@ -1,26 +1,27 @@
 // vpm_rot.cuh -- both-sides sweeps of the FP32-compensated self sums (fused velocity +
-// stretching, velocity, PSE, the LES step sums), with the source side carried around the warp
-// in registers.
+// stretching, velocity, PSE, the LES step sums, the adjoint of (u, S)), with the source side
+// carried around the warp in registers.
 //
 // The pair terms of (i <- j) and (j <- i) share r^2, the core, the rsqrt and the kernel
 // values.  Seen from particle j, with r = x_i - x_j as computed for target i:
 //   U_j += -g (r x a_i),   A_j += -g (a_j - a_i),   B_j += -h r,   h = f a_i . (r x a_j),
 //   P_j += -k (a_j - a_i)   (PSE; nu_j is applied per particle in the finalize),
 // so one evaluation of an unordered pair costs 53 FP32 lane-ops instead of 2 x 38 for the
-// fused sum, 31 instead of 2 x 22 for the velocity, 24 instead of 2 x 21 for PSE and 69-82
-// instead of 2 x 52-56 for the four LES step sums.
+// fused sum, 31 instead of 2 x 22 for the velocity, 24 instead of 2 x 21 for PSE, 69-82
+// instead of 2 x 52-56 for the four LES step sums and about 128 instead of 2 x 100 for the
+// adjoint.
 //
-// Warp layout: each lane holds four targets (two packed FP32x2 lanes) and one source of the
-// current batch of 32 (read from L2, the next batch prefetched).  In 32 steps every lane meets
-// every source of the batch: after each step the sources and their source-side accumulators
-// move one lane down (__shfl_sync), so after the 32nd step each source is back in its lane
-// with its sums over the warp's 128 targets.  Warp shuffles are the second-scarcest resource
-// here (about one per two clocks per SM); four targets per lane keep them at 25 per 256
-// ordered pairs for the fused sum.  The source-side sums are then added over the CTA's warps
+// Warp layout: each lane holds 2 kP targets (kP packed FP32x2 lanes; kP = 2 for every
+// operator here) and one source of the current batch of 32 (read from L2, the next batch
+// prefetched).  In 32 steps every lane meets every source of the batch: after each step the
+// sources and their source-side accumulators move one lane down (__shfl_sync), so after the
+// 32nd step each source is back in its lane with its sums over the warp's 64 kP targets.
+// Warp shuffles are the second-scarcest resource here (about one per two clocks per SM);
+// four targets per lane keep them at 25 per 256 ordered pairs for the fused sum.  The source-side sums are then added over the CTA's warps
 // in FP64 (fixed order) and added into the accumulator of the source particle with a
 // non-returning atomic.
 //
-// Tile-pair schedule: particles form nt tiles of T = 128 * WARPS.  A CTA owns one tile pair
+// Tile-pair schedule: particles form nt tiles of T = 64 kP WARPS.  A CTA owns one tile pair
 // (I, J), I < J.  Diagonal pair q of a launch is J - I = k (accumulator sets 4q / 4q+1 for
 // the target / source side) together with J - I = nt - k (sets 4q+2 / 4q+3): every
 // accumulator element has one writer per launch and the launches run in stream order, so the
@@ -30,17 +31,19 @@
 // order.
 //
 // Accumulation: target side in FP32 per batch of 32 sources, folded into FP64 carries held in
-// shared memory; source side in FP32 over the warp's 128 targets (each half of the packed
-// accumulator sums 64 terms), then FP64 across warps and tile pairs.
+// shared memory; source side in FP32 over the warp's 64 kP targets (each half of the packed
+// accumulator sums 32 kP terms), then FP64 across warps and tile pairs.
 #pragma once
 
+#include "vpm_adjoint.cuh"
 #include "vpm_sweep.cuh"
 
 namespace vpm {
 
 // Build parameters: warps per CTA, resident CTAs per SM the registers are sized for (fused
 // sum VPM_ROT_MINB, three-sum operators VPM_ROT3_MINB, LES step VPM_ROT15_MINB: its 77 KB of
-// shared memory allow two), unroll of the 32 steps.
+// shared memory allow two; adjoint VPM_ROTG_MINB), unroll of the 32 steps, packed target
+// lanes per thread of the adjoint (VPM_ROTG_P; the others hold two).
 #ifndef VPM_ROT_WARPS
 #define VPM_ROT_WARPS 4
 #endif
@@ -59,14 +62,96 @@ namespace vpm {
 #ifndef VPM_ROT15_UNROLL
 #define VPM_ROT15_UNROLL 2
 #endif
+#ifndef VPM_ROTG_P
+#define VPM_ROTG_P 2
+#endif
+#ifndef VPM_ROTG_MINB
+#define VPM_ROTG_MINB 2
+#endif
+#ifndef VPM_ROTG_UNROLL
+#define VPM_ROTG_UNROLL 2
+#endif
+
+constexpr int kRotWarps = VPM_ROT_WARPS;
+constexpr int kRotThreads = 32 * kRotWarps;
+constexpr float kRotFar = 1e15f;  // position of the padding sources: every kernel underflows
+
+struct RotArgs {
+  const void* rec;  // packed records of all n particles (the operator's record type)
+  int64_t n;
+  int nt;       // tiles of the operator's rot_tile particles
+  int k0;       // first diagonal of this launch (0 = the diagonal tiles)
+  double* acc;  // accumulators [sets][NV][n]
+};
+
+// Particles per tile: kP packed FP32x2 target lanes (2 kP targets) per thread.
+template <class Op>
+__host__ __device__ constexpr int rot_tile() {
+  return 64 * Op::kP * kRotWarps;
+}
+
+constexpr size_t rot_smem_bytes(int nv, int tile) {
+  return size_t(tile) * nv * sizeof(double) +               // target-side FP64 carries
+         size_t(2) * kRotWarps * 32 * nv * sizeof(float);  // source-side sums, double-buffered
+}
+
+// The source a lane holds on the standard 64-byte record: position, core, strength.
+struct RotSrc {
+  float x, y, z, s, ax, ay, az;
+};
+
+// Rotation policy of the operators on the standard record (Rec<float2>): four targets per
+// lane; the source's position, strength and (for general cores) core move around the warp.
+template <class OneSidedOp, bool UC>
+struct RotStd {
+  using V = float2;
+  using Record = Rec<float2>;
+  using OneSided = OneSidedOp;
+  using TgtT = Tgt<float2>;
+  using SrcT = Src<float2>;
+  using Lane = RotSrc;
+  static constexpr int kP = 2;
+  static constexpr bool kSrcCore = !UC;  // the pair core needs the source's sigma
+
+  // Source j of the packed records (j < n), or a padding source far away with no strength.
+  __device__ __forceinline__ static Lane load_lane(const Record* rec, int64_t j, int64_t n) {
+    if (j < n) {
+      const float4* p = reinterpret_cast<const float4*>(rec + j);
+      const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+      return Lane{a.x, a.z, b.x, b.z, c.x, c.z, d.x};
+    }
+    return Lane{kRotFar, kRotFar, kRotFar, 1.f, 0.f, 0.f, 0.f};
+  }
+  // lane l takes what lane src_lane held
+  __device__ __forceinline__ static void shuffle(Lane& c, int src_lane) {
+    c.x = __shfl_sync(0xffffffffu, c.x, src_lane);
+    c.y = __shfl_sync(0xffffffffu, c.y, src_lane);
+    c.z = __shfl_sync(0xffffffffu, c.z, src_lane);
+    if constexpr (kSrcCore) c.s = __shfl_sync(0xffffffffu, c.s, src_lane);
+    c.ax = __shfl_sync(0xffffffffu, c.ax, src_lane);
+    c.ay = __shfl_sync(0xffffffffu, c.ay, src_lane);
+    c.az = __shfl_sync(0xffffffffu, c.az, src_lane);
+  }
+  __device__ __forceinline__ static SrcT broadcast(const Lane& c) {
+    return SrcT{make_float2(c.x, c.x),   make_float2(c.y, c.y),   make_float2(c.z, c.z),
+                make_float2(c.s, c.s),   make_float2(c.ax, c.ax), make_float2(c.ay, c.ay),
+                make_float2(c.az, c.az), make_float2(0.f, 0.f)};
+  }
+  __device__ __forceinline__ static TgtT target(const Record* const* r) { return make_tgt(r); }
+  // one-sided pair of the diagonal tiles; the pair i == j adds nothing in these operators
+  __device__ __forceinline__ static void diag(const TgtT& t, V* acc, const SrcT& s,
+                                              const int64_t*, int64_t) {
+    OneSided::pair(t, acc, s, nullptr, 0);
+  }
+  // every source-side sum is carried and stored
+  __device__ __forceinline__ static constexpr bool carried(int) { return true; }
+};
 
 // Fused velocity + stretching, both sides of the pair (FP32x2 lanes).
 template <bool REFINE, bool UC>
-struct OpVelStretchBoth {
+struct OpVelStretchBoth : RotStd<OpVelStretch<float2, REFINE, UC>, UC> {
   using V = float2;
-  using OneSided = OpVelStretch<float2, REFINE, UC>;
   static constexpr int NV = 9;
-  static constexpr bool kSrcCore = !UC;  // the pair core needs the source's sigma
   static constexpr int kMinBlocks = VPM_ROT_MINB;
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
@@ -113,11 +198,9 @@ struct OpVelStretchBoth {
 
 // Self-induced velocity, both sides of the pair (FP32x2 lanes): U_j += -g (r x a_i).
 template <bool REFINE, bool UC>
-struct OpVelBoth {
+struct OpVelBoth : RotStd<OpVel<float2, REFINE, UC>, UC> {
   using V = float2;
-  using OneSided = OpVel<float2, REFINE, UC>;
   static constexpr int NV = 3;
-  static constexpr bool kSrcCore = !UC;
   static constexpr int kMinBlocks = VPM_ROT3_MINB;
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
@@ -150,11 +233,9 @@ struct OpVelBoth {
 // the exchange antisymmetric, P_j += -k (a_j - a_i); nu of each particle is applied by the
 // finalize.
 template <bool REFINE, bool UC>
-struct OpPseBoth {
+struct OpPseBoth : RotStd<OpPse<float2, REFINE, UC>, UC> {
   using V = float2;
-  using OneSided = OpPse<float2, REFINE, UC>;
   static constexpr int NV = 3;
-  static constexpr bool kSrcCore = !UC;
   static constexpr int kMinBlocks = VPM_ROT3_MINB;
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
@@ -189,11 +270,9 @@ struct OpPseBoth {
 // lane-ops per unordered pair with uniform cores, about 82 without (one-sided: 2 x 52,
 // 2 x 56).  255 registers per thread: two CTAs per SM, step loop unrolled 2.
 template <bool REFINE, bool UC>
-struct OpLesStepBoth {
+struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
   using V = float2;
-  using OneSided = OpLesStep<float2, REFINE, UC>;
   static constexpr int NV = 15;
-  static constexpr bool kSrcCore = !UC;
   static constexpr int kMinBlocks = VPM_ROT15_MINB;
   static constexpr int kUnroll = VPM_ROT15_UNROLL;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
@@ -273,46 +352,159 @@ struct OpLesStepBoth {
   }
 };
 
-struct RotArgs {
-  const Rec<float2>* rec;  // packed records of all n particles
-  int64_t n;
-  int nt;       // tiles of kRotTile particles
-  int k0;       // first diagonal of this launch (0 = the diagonal tiles)
-  double* acc;  // accumulators [sets][NV][n]
-};
+// Adjoint of the right-hand side (u, S) (OpRhsVjp, without PSE), both sides of the pair, on
+// the 160-byte adjoint record.  The gather form of OpRhsVjp already visits each pair in both
+// roles for its target k; the scalars it builds (E, D, the kernel derivatives) are symmetric
+// under k <-> l, so seen from particle l (r -> -r, w -> -w, ds -> -ds, dp unchanged):
+//   xbar_l  += -(cr r + f dp w + f d ds)                   (minus the target's term)
+//   abar_l  += -(g (r x u'_k + m_k) + f dp (r x a_k))
+//   dL/ds_l += sd,   G_a(l) += g a_k,   G_u(l) += g u'_k
+// (the G_a, G_u cross products and G_a x s'_l are applied by the same finalize pass).  About
+// 128 FP32 lane-ops per unordered pair against 2 x 100 for the gather.  The source lane
+// carries 16 values (position, core, strength, u', s', m); slot VJ_NU stays empty.
+template <bool REFINE>
+struct OpRhsVjpBoth {
+  using V = float2;
+  using Record = RecG<float2>;
+  using OneSided = OpRhsVjp<float2, REFINE, false>;
+  struct TgtT : TgtG<float2> {
+    float2 mx, my, mz;  // m_k = a_k x s'_k
+  };
+  using SrcT = SrcG<float2>;
+  struct Lane {
+    float x, y, z, s, ax, ay, az, ux, uy, uz, gx, gy, gz, mx, my, mz;
+  };
+  static constexpr int NV = OneSided::NV;
+  static constexpr int kP = VPM_ROTG_P;
+  static constexpr int kMinBlocks = VPM_ROTG_MINB;
+  static constexpr int kUnroll = VPM_ROTG_UNROLL;
 
-constexpr int kRotWarps = VPM_ROT_WARPS;
-constexpr int kRotThreads = 32 * kRotWarps;
-constexpr int kRotTile = 128 * kRotWarps;  // four targets per lane (two packed FP32x2 lanes)
-constexpr float kRotFar = 1e15f;           // position of the padding sources: g, f underflow
-
-constexpr size_t rot_smem_bytes(int nv) {
-  return size_t(kRotTile) * nv * sizeof(double) +          // target-side FP64 carries
-         size_t(2) * kRotWarps * 32 * nv * sizeof(float);  // source-side sums, double-buffered
-}
-
-struct RotSrc {
-  float x, y, z, s, ax, ay, az;
-};
-
-// Source j of the packed records (j < n), or a padding source far away with no strength.
-__device__ __forceinline__ RotSrc rot_load_src(const Rec<float2>* rec, int64_t j, int64_t n) {
-  if (j < n) {
-    const float4* p = reinterpret_cast<const float4*>(rec + j);
-    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
-    return RotSrc{a.x, a.z, b.x, b.z, c.x, c.z, d.x};
+  __device__ __forceinline__ static Lane load_lane(const Record* rec, int64_t j, int64_t n) {
+    if (j < n) {
+      const float4* p = reinterpret_cast<const float4*>(rec + j);
+      const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3),
+                   e = __ldg(p + 4), f = __ldg(p + 5), g = __ldg(p + 6), h = __ldg(p + 7),
+                   i = __ldg(p + 8);
+      return Lane{a.x, a.z, b.x, b.z, c.x, c.z, d.x, e.x, e.z, f.x, g.x, g.z, h.x, f.z, h.z, i.x};
+    }
+    return Lane{kRotFar, kRotFar, kRotFar, 1.f, 0.f, 0.f, 0.f, 0.f,
+                0.f,     0.f,     0.f,     0.f, 0.f, 0.f, 0.f, 0.f};
   }
-  return RotSrc{kRotFar, kRotFar, kRotFar, 1.f, 0.f, 0.f, 0.f};
-}
+  __device__ __forceinline__ static void shuffle(Lane& c, int src_lane) {
+    float* v = reinterpret_cast<float*>(&c);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = __shfl_sync(0xffffffffu, v[q], src_lane);
+  }
+  __device__ __forceinline__ static SrcT broadcast(const Lane& c) {
+    const auto b = [](float v) { return make_float2(v, v); };
+    return SrcT{b(c.x),  b(c.y),  b(c.z),  b(c.s),  b(c.ax), b(c.ay), b(c.az), b(0.f), b(c.ux),
+                b(c.uy), b(c.uz), b(c.gx), b(c.gy), b(c.gz), b(c.mx), b(c.my), b(c.mz)};
+  }
+  __device__ __forceinline__ static TgtT target(const Record* const* r) {
+    TgtT t;
+    static_cast<TgtG<float2>&>(t) = make_tgtg(r);
+    t.mx = make_float2(r[0]->mx.x, r[1]->mx.x);
+    t.my = make_float2(r[0]->my.x, r[1]->my.x);
+    t.mz = make_float2(r[0]->mz.x, r[1]->mz.x);
+    return t;
+  }
+  // diagonal tiles: the gather operator, with the pair k == l excluded by index
+  __device__ __forceinline__ static void diag(const TgtT& t, V* acc, const SrcT& s,
+                                              const int64_t* ti, int64_t j) {
+    OneSided::pair(t, acc, s, ti, j);
+  }
+  __device__ __forceinline__ static constexpr bool carried(int v) { return v != VJ_NU; }
+
+  __device__ __forceinline__ static void pair2(const TgtT& t, V* acc, V* jv, const SrcT& s) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    const V sg = fma(s.s, splat<V>(0.5), t.hs);
+    const V s2 = sg * sg;
+    const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
+    const V y = rsqrt_lane<REFINE>(x);
+    const V y2 = y * y;
+    const V y5 = (y2 * y2) * y;
+    const V y7 = y5 * y2;
+    const V y9 = y7 * y2;
+    const V s3 = s2 * sg;
+    const V t1 = fma(splat<V>(1.5), s2, x);
+    const V g = t1 * y5;
+    const V t2 = t1 + s2;
+    const V f = splat<V>(3.0) * (t2 * y7);
+    const V gs = splat<V>(-7.5) * (s3 * y7);           // dg/ds
+    const V f2r = splat<V>(-15.0) * ((t2 + s2) * y9);  // 2 df/dr^2
+    const V fs = splat<V>(-52.5) * (s3 * y9);          // df/ds
+    const V clx = fma(ry, s.az, -(rz * s.ay));  // r x a_l
+    const V cly = fma(rz, s.ax, -(rx * s.az));
+    const V clz = fma(rx, s.ay, -(ry * s.ax));
+    const V ckx = fma(ry, t.az, -(rz * t.ay));  // r x a_k
+    const V cky = fma(rz, t.ax, -(rx * t.az));
+    const V ckz = fma(rx, t.ay, -(ry * t.ax));
+    const V wx = fma(s.ay, t.az, -(s.az * t.ay));  // w = a_l x a_k
+    const V wy = fma(s.az, t.ax, -(s.ax * t.az));
+    const V wz = fma(s.ax, t.ay, -(s.ay * t.ax));
+    const V dsx = t.gx - s.gx, dsy = t.gy - s.gy, dsz = t.gz - s.gz;
+    const V eT = fma(t.ux, clx, fma(t.uy, cly, t.uz * clz));
+    const V eS = fma(s.ux, ckx, fma(s.uy, cky, s.uz * ckz));
+    const V dsw = fma(dsx, wx, fma(dsy, wy, dsz * wz));
+    const V E = (eT - eS) - dsw;
+    const V d = fma(rx, wx, fma(ry, wy, rz * wz));
+    const V dp = fma(dsx, rx, fma(dsy, ry, dsz * rz));
+    const V D = d * dp;
+    const V cr = fma(f2r, D, -(f * E));  // 2 dg/dr^2 E + 2 df/dr^2 D  (-2 dg/dr^2 = f)
+    const V sd = fma(gs, E, fs * D);
+    const V fdp = f * dp;
+    const V fd = f * d;
+    const V px = fma(cr, rx, fma(fdp, wx, fd * dsx));
+    const V py = fma(cr, ry, fma(fdp, wy, fd * dsy));
+    const V pz = fma(cr, rz, fma(fdp, wz, fd * dsz));
+    acc[VJ_X + 0] = acc[VJ_X + 0] + px;
+    acc[VJ_X + 1] = acc[VJ_X + 1] + py;
+    acc[VJ_X + 2] = acc[VJ_X + 2] + pz;
+    acc[VJ_S] = acc[VJ_S] + sd;
+    acc[VJ_GA + 0] = fma(g, s.ax, acc[VJ_GA + 0]);
+    acc[VJ_GA + 1] = fma(g, s.ay, acc[VJ_GA + 1]);
+    acc[VJ_GA + 2] = fma(g, s.az, acc[VJ_GA + 2]);
+    acc[VJ_GU + 0] = fma(g, s.ux, acc[VJ_GU + 0]);
+    acc[VJ_GU + 1] = fma(g, s.uy, acc[VJ_GU + 1]);
+    acc[VJ_GU + 2] = fma(g, s.uz, acc[VJ_GU + 2]);
+    const V nx = fma(ry, s.uz, -(rz * s.uy)) - s.mx;  // r x u'_l - m_l
+    const V ny = fma(rz, s.ux, -(rx * s.uz)) - s.my;
+    const V nz = fma(rx, s.uy, -(ry * s.ux)) - s.mz;
+    acc[VJ_A + 0] = fma(g, nx, fma(fdp, clx, acc[VJ_A + 0]));
+    acc[VJ_A + 1] = fma(g, ny, fma(fdp, cly, acc[VJ_A + 1]));
+    acc[VJ_A + 2] = fma(g, nz, fma(fdp, clz, acc[VJ_A + 2]));
+    // source side, every sum with the opposite sign (negated when it is stored)
+    jv[VJ_X + 0] = jv[VJ_X + 0] + px;
+    jv[VJ_X + 1] = jv[VJ_X + 1] + py;
+    jv[VJ_X + 2] = jv[VJ_X + 2] + pz;
+    jv[VJ_S] = jv[VJ_S] - sd;
+    jv[VJ_GA + 0] = fma(-g, t.ax, jv[VJ_GA + 0]);
+    jv[VJ_GA + 1] = fma(-g, t.ay, jv[VJ_GA + 1]);
+    jv[VJ_GA + 2] = fma(-g, t.az, jv[VJ_GA + 2]);
+    jv[VJ_GU + 0] = fma(-g, t.ux, jv[VJ_GU + 0]);
+    jv[VJ_GU + 1] = fma(-g, t.uy, jv[VJ_GU + 1]);
+    jv[VJ_GU + 2] = fma(-g, t.uz, jv[VJ_GU + 2]);
+    const V qx = fma(ry, t.uz, -(rz * t.uy)) + t.mx;  // r x u'_k + m_k
+    const V qy = fma(rz, t.ux, -(rx * t.uz)) + t.my;
+    const V qz = fma(rx, t.uy, -(ry * t.ux)) + t.mz;
+    jv[VJ_A + 0] = fma(g, qx, fma(fdp, ckx, jv[VJ_A + 0]));
+    jv[VJ_A + 1] = fma(g, qy, fma(fdp, cky, jv[VJ_A + 1]));
+    jv[VJ_A + 2] = fma(g, qz, fma(fdp, ckz, jv[VJ_A + 2]));
+  }
+};
 
 template <class Op, bool DIAG>
 __global__ void __launch_bounds__(kRotThreads, Op::kMinBlocks)
 rot_sweep_kernel(const RotArgs a) {
+  using Record = typename Op::Record;
+  using Lane = typename Op::Lane;
   constexpr int NV = Op::NV;
-  constexpr int T = kRotTile;
+  constexpr int P = Op::kP;
+  constexpr int T = rot_tile<Op>();
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* car = reinterpret_cast<double*>(smem_raw);  // [NV][T]
   float* jbuf = reinterpret_cast<float*>(smem_raw + size_t(T) * NV * sizeof(double));
+  const Record* rec = static_cast<const Record*>(a.rec);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int I, J, set_i, set_j;
@@ -342,66 +534,61 @@ rot_sweep_kernel(const RotArgs a) {
 
   for (int q = tid; q < T * NV; q += kRotThreads) car[q] = 0.0;
 
-  // this lane's four targets: warp*128 + lane + {0, 32} (first packed lane) and + {64, 96}
-  int lt[4];
-  typename Op::OneSided::TgtT tg[2];
+  // this lane's targets: packed lane p holds warp * 64P + 64p + lane + {0, 32}
+  int lt[2 * P];
+  typename Op::TgtT tg[P];
 #pragma unroll
-  for (int p = 0; p < 2; ++p) {
-    lt[2 * p] = warp * 128 + p * 64 + lane;
+  for (int p = 0; p < P; ++p) {
+    lt[2 * p] = warp * 64 * P + p * 64 + lane;
     lt[2 * p + 1] = lt[2 * p] + 32;
     const int64_t t0 = i0 + lt[2 * p], t1 = i0 + lt[2 * p + 1];
-    const Rec<float2>* recs[2] = {a.rec + (t0 < a.n ? t0 : a.n - 1),
-                                  a.rec + (t1 < a.n ? t1 : a.n - 1)};
-    tg[p] = make_tgt(recs);
+    const Record* recs[2] = {rec + (t0 < a.n ? t0 : a.n - 1), rec + (t1 < a.n ? t1 : a.n - 1)};
+    tg[p] = Op::target(recs);
   }
-  float2 acc[2][NV];
+  float2 acc[P][NV];
 #pragma unroll
-  for (int p = 0; p < 2; ++p)
+  for (int p = 0; p < P; ++p)
 #pragma unroll
     for (int v = 0; v < NV; ++v) acc[p][v] = make_float2(0.f, 0.f);
   __syncthreads();  // carries zeroed
 
   const int nb = (cnt + 31) / 32;
-  RotSrc nxt = rot_load_src(a.rec, j0 + lane, j0 + cnt);
+  Lane nxt = Op::load_lane(rec, j0 + lane, j0 + cnt);
   for (int b = 0; b < nb; ++b) {
-    RotSrc cur = nxt;  // the source this lane holds at step 0
-    if (b + 1 < nb) nxt = rot_load_src(a.rec, j0 + (b + 1) * 32 + lane, j0 + cnt);
+    Lane cur = nxt;  // the source this lane holds at step 0
+    if (b + 1 < nb) nxt = Op::load_lane(rec, j0 + (b + 1) * 32 + lane, j0 + cnt);
     float2 jv[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) jv[v] = make_float2(0.f, 0.f);
     const int src_lane = (lane + 1) & 31;
 #pragma unroll Op::kUnroll
     for (int step = 0; step < 32; ++step) {
-      const Src<float2> src{make_float2(cur.x, cur.x),   make_float2(cur.y, cur.y),
-                            make_float2(cur.z, cur.z),   make_float2(cur.s, cur.s),
-                            make_float2(cur.ax, cur.ax), make_float2(cur.ay, cur.ay),
-                            make_float2(cur.az, cur.az), make_float2(0.f, 0.f)};
+      const typename Op::SrcT src = Op::broadcast(cur);
 #pragma unroll
-      for (int p = 0; p < 2; ++p) {
-        if constexpr (DIAG)
-          Op::OneSided::pair(tg[p], acc[p], src, nullptr, 0);
-        else
+      for (int p = 0; p < P; ++p) {
+        if constexpr (DIAG) {
+          // at this step the lane holds source b * 32 + ((lane + step) mod 32) of the tile
+          const int64_t ti[2] = {i0 + lt[2 * p], i0 + lt[2 * p + 1]};
+          Op::diag(tg[p], acc[p], src, ti, j0 + b * 32 + ((lane + step) & 31));
+        } else {
           Op::pair2(tg[p], acc[p], jv, src);
+        }
       }
       // pass the source (and its sums) one lane down: lane l now holds what lane l+1 held
-      cur.x = __shfl_sync(0xffffffffu, cur.x, src_lane);
-      cur.y = __shfl_sync(0xffffffffu, cur.y, src_lane);
-      cur.z = __shfl_sync(0xffffffffu, cur.z, src_lane);
-      if constexpr (Op::kSrcCore) cur.s = __shfl_sync(0xffffffffu, cur.s, src_lane);
-      cur.ax = __shfl_sync(0xffffffffu, cur.ax, src_lane);
-      cur.ay = __shfl_sync(0xffffffffu, cur.ay, src_lane);
-      cur.az = __shfl_sync(0xffffffffu, cur.az, src_lane);
+      Op::shuffle(cur, src_lane);
       if constexpr (!DIAG) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-          jv[v].x = __shfl_sync(0xffffffffu, jv[v].x, src_lane);
-          jv[v].y = __shfl_sync(0xffffffffu, jv[v].y, src_lane);
+          if (Op::carried(v)) {
+            jv[v].x = __shfl_sync(0xffffffffu, jv[v].x, src_lane);
+            jv[v].y = __shfl_sync(0xffffffffu, jv[v].y, src_lane);
+          }
         }
       }
     }
     // target side: this batch's FP32 sums into the FP64 carries (each thread its own rows)
 #pragma unroll
-    for (int p = 0; p < 2; ++p) {
+    for (int p = 0; p < P; ++p) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         car[v * T + lt[2 * p]] += double(acc[p][v].x);
@@ -418,6 +605,7 @@ rot_sweep_kernel(const RotArgs a) {
       const int nsrc = (cnt - b * 32 < 32) ? cnt - b * 32 : 32;
       for (int q = tid; q < nsrc * NV; q += kRotThreads) {
         const int jj = q / NV, v = q - jj * NV;
+        if (!Op::carried(v)) continue;
         double sum = 0.0;
 #pragma unroll
         for (int w = 0; w < kRotWarps; ++w) sum += double(jb[(w * 32 + jj) * NV + v]);
