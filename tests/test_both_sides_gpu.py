@@ -1,6 +1,7 @@
 """The both-sides sweeps of the FP32-compensated self sums (fused velocity + stretching,
-velocity, PSE, the LES step sums, the adjoint of (u, S); csrc/vpm_rot.cuh), forced on at small sizes so that two, three and many tiles, odd and even
-tile counts, several diagonal pairs per launch and a ragged last tile are covered: against
+velocity, PSE, the LES step sums, the adjoint of (u, S); csrc/vpm_rot.cuh), forced on at
+small sizes so that two, three and many tiles, odd and even tile counts, several diagonal
+pairs per launch, a ragged last tile and a last tile of one particle are covered: against
 the FP64 one-sided sweep (itself pinned to the reference), against the FP32 one-sided sweep,
 and bitwise repeatable."""
 import numpy as np
@@ -36,8 +37,8 @@ def _dev32(f):
             for z in (f.positions, f.strengths, f.radii)]
 
 
-@pytest.mark.parametrize("n,ring", [(1000, False), (1536, False), (3001, False), (2048, True),
-                                    (4096, True), (20000, False)])
+@pytest.mark.parametrize("n,ring", [(513, False), (1000, False), (1536, False), (3001, False),
+                                    (2048, True), (4096, True), (20000, False)])
 @pytest.mark.parametrize("uniform_core", [False, True])
 def test_both_sides_vs_fp64(n, ring, uniform_core):
     from openonda_b200 import kernels
@@ -111,8 +112,8 @@ def test_records_whole_set_and_shards(both_sides_always):
         assert normwise(joined.cpu().numpy(), ref[k].cpu().numpy()) <= tol
 
 
-@pytest.mark.parametrize("n,ring", [(1000, False), (1536, False), (3001, False), (2048, True),
-                                    (4096, True), (20000, False)])
+@pytest.mark.parametrize("n,ring", [(513, False), (1000, False), (1536, False), (3001, False),
+                                    (2048, True), (4096, True), (20000, False)])
 @pytest.mark.parametrize("uniform_core", [False, True])
 @pytest.mark.parametrize("op", ["selfinduced_velocity", "strength_gradients_pse"])
 def test_velocity_and_pse_both_sides_vs_fp64(op, n, ring, uniform_core):
@@ -158,8 +159,8 @@ def test_helicity_and_shards_stay_one_sided(both_sides_always):
     assert kernels.sweep_launches("strength_gradients_pse", "fp32c", n, n) > 3
 
 
-@pytest.mark.parametrize("n,ring", [(1000, False), (3001, False), (2048, True), (4096, True),
-                                    (20000, False)])
+@pytest.mark.parametrize("n,ring", [(513, False), (1000, False), (3001, False), (2048, True),
+                                    (4096, True), (20000, False)])
 @pytest.mark.parametrize("uniform_core", [False, True])
 def test_les_step_sums_both_sides_vs_fp64(n, ring, uniform_core):
     """The four LES step sums (velocity, stretching, particle vorticity with the source core,
@@ -196,8 +197,8 @@ def test_les_step_sums_both_sides_vs_fp64(n, ring, uniform_core):
     assert kernels.device_errors() == 0
 
 
-@pytest.mark.parametrize("n,ring", [(1000, False), (3001, False), (2048, True), (4096, True),
-                                    (20000, False)])
+@pytest.mark.parametrize("n,ring", [(513, False), (1000, False), (3001, False), (2048, True),
+                                    (4096, True), (20000, False)])
 def test_rhs_vjp_both_sides_vs_fp64(n, ring):
     """The adjoint of (u, S) on the both-sides schedule (each pair's derivative terms once for
     both particles) against the FP64 gather adjoint, no worse than the FP32c gather, and
