@@ -586,7 +586,8 @@ struct Ops {
   using VelBoth = OpVelBoth<REFINE, UC>;                // FP32 only
   using PseBoth = OpPseBoth<REFINE, UC>;                // FP32 only
   using LesStepBoth = OpLesStepBoth<REFINE, UC>;        // FP32 only
-  using RhsVjpBoth = OpRhsVjpBoth<REFINE>;              // FP32 only
+  using RhsVjpBoth = OpRhsVjpBoth<REFINE, false>;       // FP32 only
+  using RhsVjpPseBoth = OpRhsVjpBoth<REFINE, true>;     // FP32 only
   using RhsVjp = OpRhsVjp<T, REFINE, false>;
   using RhsVjpPse = OpRhsVjp<T, REFINE, true>;
   using KeGrad = OpKeGrad<T, REFINE>;
@@ -641,6 +642,10 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
       }
       return Sweep<typename O::RhsVjp, T>::plan(m, n, p, mpb);
     case VPM_OP_RHS_VJP_PSE:
+      if constexpr (LaneTraits<T>::kLanes == 2) {
+        if (RotSweep<typename O::RhsVjpPseBoth>::usable(m, n, mpb))
+          return RotSweep<typename O::RhsVjpPseBoth>::plan(n, p, mpb);
+      }
       return Sweep<typename O::RhsVjpPse, T>::plan(m, n, p, mpb);
     case VPM_OP_KINETIC_ENERGY_GRAD:
       return Sweep<typename O::KeGrad, T>::plan(m, n, p, mpb);
@@ -936,7 +941,12 @@ int run_grad(const GradCall& c) {
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "pack launch");
   if (c.op == VPM_OP_RHS_VJP_PSE) {
-    rc = Sweep<typename O::RhsVjpPse, T>::launch(p, rec, c.n, 0, rec, c.n, part, c.st);
+    rc = VPM_OK;
+    if constexpr (LaneTraits<T>::kLanes == 2) {
+      if (p.pairs) rc = RotSweep<typename O::RhsVjpPseBoth>::launch(p, rec, c.n, part, c.st);
+    }
+    if (!p.pairs)
+      rc = Sweep<typename O::RhsVjpPse, T>::launch(p, rec, c.n, 0, rec, c.n, part, c.st);
     if (rc) return rc;
     finalize_vjp_kernel<T, O::RhsVjpPse::NV, true>
         <<<blocks, 256, 0, c.st>>>(part, p.splits, c.n, rec, c.ox, c.oa, c.os, c.onu);

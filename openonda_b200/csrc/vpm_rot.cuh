@@ -71,6 +71,15 @@ namespace vpm {
 #ifndef VPM_ROTG_UNROLL
 #define VPM_ROTG_UNROLL 2
 #endif
+#ifndef VPM_ROTGP_P
+#define VPM_ROTGP_P 1
+#endif
+#ifndef VPM_ROTGP_MINB
+#define VPM_ROTGP_MINB 2
+#endif
+#ifndef VPM_ROTGP_UNROLL
+#define VPM_ROTGP_UNROLL 2
+#endif
 
 constexpr int kRotWarps = VPM_ROT_WARPS;
 constexpr int kRotThreads = 32 * kRotWarps;
@@ -352,8 +361,8 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
   }
 };
 
-// Adjoint of the right-hand side (u, S) (OpRhsVjp, without PSE), both sides of the pair, on
-// the 160-byte adjoint record.  The gather form of OpRhsVjp already visits each pair in both
+// Adjoint of the right-hand side (u, S [+ P]) (OpRhsVjp), both sides of the pair, on the
+// 160-byte adjoint record.  The gather form of OpRhsVjp already visits each pair in both
 // roles for its target k; the scalars it builds (E, D, the kernel derivatives) are symmetric
 // under k <-> l, so seen from particle l (r -> -r, w -> -w, ds -> -ds, dp unchanged):
 //   xbar_l  += -(cr r + f dp w + f d ds)                   (minus the target's term)
@@ -362,22 +371,27 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
 // (the G_a, G_u cross products and G_a x s'_l are applied by the same finalize pass).  About
 // 128 FP32 lane-ops per unordered pair against 2 x 100 for the gather.  The source lane
 // carries 16 values (position, core, strength, u', s', m); slot VJ_NU stays empty.
-template <bool REFINE>
+// With PSE the exchange scalar Q = nu'_k s'_k.(a_l - a_k) + nu'_l s'_l.(a_k - a_l) is
+// symmetric too, and particle l takes dL/dnu'_l += k s'_l.(a_k - a_l), sum k and
+// sum k nu'_k s'_k; the lane carries nu' as a 17th value.  The 18 sums fit two targets per
+// lane (VPM_ROTGP_P).
+template <bool REFINE, bool PSE>
 struct OpRhsVjpBoth {
   using V = float2;
   using Record = RecG<float2>;
-  using OneSided = OpRhsVjp<float2, REFINE, false>;
+  using OneSided = OpRhsVjp<float2, REFINE, PSE>;
   struct TgtT : TgtG<float2> {
     float2 mx, my, mz;  // m_k = a_k x s'_k
   };
   using SrcT = SrcG<float2>;
   struct Lane {
-    float x, y, z, s, ax, ay, az, ux, uy, uz, gx, gy, gz, mx, my, mz;
+    float x, y, z, s, ax, ay, az, ux, uy, uz, gx, gy, gz, mx, my, mz, nu;  // nu: 105 nu
   };
+  static constexpr int kLaneValues = PSE ? 17 : 16;  // values that move around the warp
   static constexpr int NV = OneSided::NV;
-  static constexpr int kP = VPM_ROTG_P;
-  static constexpr int kMinBlocks = VPM_ROTG_MINB;
-  static constexpr int kUnroll = VPM_ROTG_UNROLL;
+  static constexpr int kP = PSE ? VPM_ROTGP_P : VPM_ROTG_P;
+  static constexpr int kMinBlocks = PSE ? VPM_ROTGP_MINB : VPM_ROTG_MINB;
+  static constexpr int kUnroll = PSE ? VPM_ROTGP_UNROLL : VPM_ROTG_UNROLL;
 
   __device__ __forceinline__ static Lane load_lane(const Record* rec, int64_t j, int64_t n) {
     if (j < n) {
@@ -385,20 +399,22 @@ struct OpRhsVjpBoth {
       const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3),
                    e = __ldg(p + 4), f = __ldg(p + 5), g = __ldg(p + 6), h = __ldg(p + 7),
                    i = __ldg(p + 8);
-      return Lane{a.x, a.z, b.x, b.z, c.x, c.z, d.x, e.x, e.z, f.x, g.x, g.z, h.x, f.z, h.z, i.x};
+      return Lane{a.x, a.z, b.x, b.z, c.x, c.z, d.x, e.x, e.z,
+                  f.x, g.x, g.z, h.x, f.z, h.z, i.x, d.z};
     }
-    return Lane{kRotFar, kRotFar, kRotFar, 1.f, 0.f, 0.f, 0.f, 0.f,
+    return Lane{kRotFar, kRotFar, kRotFar, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f,
                 0.f,     0.f,     0.f,     0.f, 0.f, 0.f, 0.f, 0.f};
   }
   __device__ __forceinline__ static void shuffle(Lane& c, int src_lane) {
     float* v = reinterpret_cast<float*>(&c);
 #pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = __shfl_sync(0xffffffffu, v[q], src_lane);
+    for (int q = 0; q < kLaneValues; ++q) v[q] = __shfl_sync(0xffffffffu, v[q], src_lane);
   }
   __device__ __forceinline__ static SrcT broadcast(const Lane& c) {
     const auto b = [](float v) { return make_float2(v, v); };
-    return SrcT{b(c.x),  b(c.y),  b(c.z),  b(c.s),  b(c.ax), b(c.ay), b(c.az), b(0.f), b(c.ux),
-                b(c.uy), b(c.uz), b(c.gx), b(c.gy), b(c.gz), b(c.mx), b(c.my), b(c.mz)};
+    return SrcT{b(c.x),  b(c.y),  b(c.z),  b(c.s),  b(c.ax), b(c.ay),
+                b(c.az), b(PSE ? c.nu : 0.f),       b(c.ux), b(c.uy), b(c.uz),
+                b(c.gx), b(c.gy), b(c.gz), b(c.mx), b(c.my), b(c.mz)};
   }
   __device__ __forceinline__ static TgtT target(const Record* const* r) {
     TgtT t;
@@ -413,7 +429,7 @@ struct OpRhsVjpBoth {
                                               const int64_t* ti, int64_t j) {
     OneSided::pair(t, acc, s, ti, j);
   }
-  __device__ __forceinline__ static constexpr bool carried(int v) { return v != VJ_NU; }
+  __device__ __forceinline__ static constexpr bool carried(int v) { return PSE || v != VJ_NU; }
 
   __device__ __forceinline__ static void pair2(const TgtT& t, V* acc, V* jv, const SrcT& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -450,8 +466,36 @@ struct OpRhsVjpBoth {
     const V d = fma(rx, wx, fma(ry, wy, rz * wz));
     const V dp = fma(dsx, rx, fma(dsy, ry, dsz * rz));
     const V D = d * dp;
-    const V cr = fma(f2r, D, -(f * E));  // 2 dg/dr^2 E + 2 df/dr^2 D  (-2 dg/dr^2 = f)
-    const V sd = fma(gs, E, fs * D);
+    V cr = fma(f2r, D, -(f * E));  // 2 dg/dr^2 E + 2 df/dr^2 D  (-2 dg/dr^2 = f)
+    V sd = fma(gs, E, fs * D);
+    if constexpr (PSE) {
+      const V z = sg * y;
+      const V z2 = z * z;
+      const V z6 = (z2 * z2) * z2;
+      const V k = (z6 * z) * y2;                      // s^7 y^9
+      const V k2r = splat<V>(-9.0) * (k * y2);        // 2 dk/dr^2
+      const V r2 = x - s2;
+      const V ks = (z6 * y2) * y2 * y * fma(splat<V>(7.0), r2, splat<V>(-2.0) * s2);  // dk/ds
+      const V ddx = s.ax - t.ax, ddy = s.ay - t.ay, ddz = s.az - t.az;  // a_l - a_k
+      const V qT = fma(t.gx, ddx, fma(t.gy, ddy, t.gz * ddz));
+      const V qS = fma(s.gx, ddx, fma(s.gy, ddy, s.gz * ddz));
+      const V Q = fma(t.nu, qT, -(s.nu * qS));
+      cr = fma(k2r, Q, cr);
+      sd = fma(ks, Q, sd);
+      acc[VJ_NU] = fma(k, qT, acc[VJ_NU]);
+      acc[VJ_K] = acc[VJ_K] + k;
+      const V kn = k * s.nu;
+      acc[VJ_KS + 0] = fma(kn, s.gx, acc[VJ_KS + 0]);
+      acc[VJ_KS + 1] = fma(kn, s.gy, acc[VJ_KS + 1]);
+      acc[VJ_KS + 2] = fma(kn, s.gz, acc[VJ_KS + 2]);
+      // source side (negated when stored): k s'_l.(a_k - a_l) = -k qS, sum k, sum k nu'_k s'_k
+      jv[VJ_NU] = fma(k, qS, jv[VJ_NU]);
+      jv[VJ_K] = jv[VJ_K] - k;
+      const V knt = k * t.nu;
+      jv[VJ_KS + 0] = fma(-knt, t.gx, jv[VJ_KS + 0]);
+      jv[VJ_KS + 1] = fma(-knt, t.gy, jv[VJ_KS + 1]);
+      jv[VJ_KS + 2] = fma(-knt, t.gz, jv[VJ_KS + 2]);
+    }
     const V fdp = f * dp;
     const V fd = f * d;
     const V px = fma(cr, rx, fma(fdp, wx, fd * dsx));

@@ -199,31 +199,34 @@ def test_les_step_sums_both_sides_vs_fp64(n, ring, uniform_core):
 
 @pytest.mark.parametrize("n,ring", [(513, False), (1000, False), (3001, False), (2048, True),
                                     (4096, True), (20000, False)])
-def test_rhs_vjp_both_sides_vs_fp64(n, ring):
-    """The adjoint of (u, S) on the both-sides schedule (each pair's derivative terms once for
-    both particles) against the FP64 gather adjoint, no worse than the FP32c gather, and
-    bitwise repeatable."""
+@pytest.mark.parametrize("pse", [False, True])
+def test_rhs_vjp_both_sides_vs_fp64(n, ring, pse):
+    """The adjoint of (u, S [+ P]) on the both-sides schedule (each pair's derivative terms
+    once for both particles) against the FP64 gather adjoint, no worse than the FP32c
+    gather, and bitwise repeatable; with PSE the viscosity gradient as well."""
     from openonda_b200 import autodiff, kernels
 
     f = _field(n, 13 + n, ring)
     x, a, s = _dev32(f)
+    nu = torch.from_numpy(np.ascontiguousarray(f.viscosities)).cuda() if pse else None
     rng = np.random.default_rng(n)
     gu = torch.from_numpy(rng.normal(size=(n, 3))).cuda()
     gs = torch.from_numpy(rng.normal(size=(n, 3))).cuda()
+    op = "rhs_vjp_pse" if pse else "rhs_vjp"
     prev = kernels.set_symmetric_min_n(1 << 40)
     try:
-        one32 = autodiff.rhs_vjp(x, a, s, None, gu, gs, "fp32c")
-        ref = autodiff.rhs_vjp(x, a, s, None, gu, gs, "fp64")
+        one32 = autodiff.rhs_vjp(x, a, s, nu, gu, gs, "fp32c")
+        ref = autodiff.rhs_vjp(x, a, s, nu, gu, gs, "fp64")
         kernels.set_symmetric_min_n(0)
-        assert kernels.sweep_launches("rhs_vjp", "fp32c", n, n) > 3  # the both-sides plan
-        both = autodiff.rhs_vjp(x, a, s, None, gu, gs, "fp32c")
-        again = autodiff.rhs_vjp(x, a, s, None, gu, gs, "fp32c")
+        assert kernels.sweep_launches(op, "fp32c", n, n) > 3  # the both-sides plan
+        both = autodiff.rhs_vjp(x, a, s, nu, gu, gs, "fp32c")
+        again = autodiff.rhs_vjp(x, a, s, nu, gu, gs, "fp32c")
     finally:
         kernels.set_symmetric_min_n(prev)
-    for k in range(3):
+    for k in range(4 if pse else 3):
         e_both = normwise(both[k].cpu().numpy(), ref[k].cpu().numpy())
         e_one = normwise(one32[k].cpu().numpy(), ref[k].cpu().numpy())
-        print(f"vjp n={n} ring={ring} k={k}: both {e_both:.2e} one {e_one:.2e}")
+        print(f"vjp pse={pse} n={n} ring={ring} k={k}: both {e_both:.2e} one {e_one:.2e}")
         assert e_both <= max(1e-5, 1.5 * e_one), (k, e_both, e_one)
         assert torch.equal(both[k], again[k])
     assert kernels.device_errors() == 0
