@@ -147,7 +147,8 @@ struct RotStd {
                 make_float2(c.az, c.az), make_float2(0.f, 0.f)};
   }
   __device__ __forceinline__ static TgtT target(const Record* const* r) { return make_tgt(r); }
-  // one-sided pair of the diagonal tiles; the pair i == j adds nothing in these operators
+  // one-sided pair of the diagonal tiles; these operators need no index for the pair i == j
+  // (it adds nothing, except the enstrophy filter sum, which includes it as the reference does)
   __device__ __forceinline__ static void diag(const TgtT& t, V* acc, const SrcT& s,
                                               const int64_t*, int64_t) {
     OneSided::pair(t, acc, s, nullptr, 0);
