@@ -230,3 +230,38 @@ def test_rhs_vjp_both_sides_vs_fp64(n, ring, pse):
         assert e_both <= max(1e-5, 1.5 * e_one), (k, e_both, e_one)
         assert torch.equal(both[k], again[k])
     assert kernels.device_errors() == 0
+
+
+def test_refined_rsqrt_both_sides(both_sides_always):
+    """The Newton-refined precision ("fp32c_refined") takes the same both-sides kernels:
+    every self sum and the adjoint stay at the FP32c bar against FP64."""
+    from openonda_b200 import autodiff, kernels
+
+    n = 3001
+    f = _field(n, 17)
+    x, a, s = _dev32(f)
+    nu = torch.from_numpy(np.ascontiguousarray(f.viscosities)).cuda()
+    p = "fp32c_refined"
+    assert kernels.sweep_launches("velocity_and_strength_gradients", p, n, n) > 3
+    pairs = [
+        (kernels.velocity_and_strength_gradients(x, a, s, precision=p),
+         kernels.velocity_and_strength_gradients(x, a, s, precision="fp64"), (1e-6, 5e-6)),
+        ((kernels.selfinduced_velocity(x, a, s, precision=p),),
+         (kernels.selfinduced_velocity(x, a, s, precision="fp64"),), (1e-6,)),
+        ((kernels.strength_gradients_pse(x, a, s, nu, precision=p),),
+         (kernels.strength_gradients_pse(x, a, s, nu, precision="fp64"),), (1e-6,)),
+        (kernels.les_step_sums(x, a, s, precision=p)[:3],
+         kernels.les_step_sums(x, a, s, precision="fp64")[:3], (1e-6, 5e-6, 1e-6)),
+    ]
+    for got, ref, tols in pairs:
+        for g, r, tol in zip(got, ref, tols):
+            assert normwise(g.cpu().numpy(), r.cpu().numpy()) <= tol
+    rng = np.random.default_rng(5)
+    gu = torch.from_numpy(rng.normal(size=(n, 3))).cuda()
+    gs = torch.from_numpy(rng.normal(size=(n, 3))).cuda()
+    for v in (None, nu):
+        got = autodiff.rhs_vjp(x, a, s, v, gu, gs, p)
+        ref = autodiff.rhs_vjp(x, a, s, v, gu, gs, "fp64")
+        for k in range(3):
+            assert normwise(got[k].cpu().numpy(), ref[k].cpu().numpy()) <= 1e-5
+    assert kernels.device_errors() == 0
