@@ -53,6 +53,12 @@ namespace vpm {
 #ifndef VPM_ROT3_MINB
 #define VPM_ROT3_MINB 3
 #endif
+#ifndef VPM_ROT_P
+#define VPM_ROT_P 3
+#endif
+#ifndef VPM_ROT3_P
+#define VPM_ROT3_P 3
+#endif
 #ifndef VPM_ROT15_MINB
 #define VPM_ROT15_MINB 2
 #endif
@@ -162,6 +168,7 @@ template <bool REFINE, bool UC>
 struct OpVelStretchBoth : RotStd<OpVelStretch<float2, REFINE, UC>, UC> {
   using V = float2;
   static constexpr int NV = 9;
+  static constexpr int kP = VPM_ROT_P;
   static constexpr int kMinBlocks = VPM_ROT_MINB;
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
@@ -211,6 +218,7 @@ template <bool REFINE, bool UC>
 struct OpVelBoth : RotStd<OpVel<float2, REFINE, UC>, UC> {
   using V = float2;
   static constexpr int NV = 3;
+  static constexpr int kP = VPM_ROT3_P;
   static constexpr int kMinBlocks = VPM_ROT3_MINB;
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
@@ -246,6 +254,7 @@ template <bool REFINE, bool UC>
 struct OpPseBoth : RotStd<OpPse<float2, REFINE, UC>, UC> {
   using V = float2;
   static constexpr int NV = 3;
+  static constexpr int kP = VPM_ROT3_P;
   static constexpr int kMinBlocks = VPM_ROT3_MINB;
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
