@@ -11,15 +11,16 @@
 // instead of 2 x 52-56 for the four LES step sums and about 128 instead of 2 x 100 for the
 // adjoint.
 //
-// Warp layout: each lane holds 2 kP targets (kP packed FP32x2 lanes; kP = 2 for every
-// operator here) and one source of the current batch of 32 (read from L2, the next batch
-// prefetched).  In 32 steps every lane meets every source of the batch: after each step the
-// sources and their source-side accumulators move one lane down (__shfl_sync), so after the
-// 32nd step each source is back in its lane with its sums over the warp's 64 kP targets.
-// Warp shuffles are the second-scarcest resource here (about one per two clocks per SM);
-// four targets per lane keep them at 25 per 256 ordered pairs for the fused sum.  The source-side sums are then added over the CTA's warps
-// in FP64 (fixed order) and added into the accumulator of the source particle with a
-// non-returning atomic.
+// Warp layout: each lane holds 2 kP targets (kP packed FP32x2 lanes: 3 for the fused,
+// velocity and PSE sums, 2 for the LES sums and the adjoint, 1 for the adjoint with PSE) and
+// one source of the current batch of 32 (read from L2, the next batch prefetched).  In 32
+// steps every lane meets every source of the batch: after each step the sources and their
+// source-side accumulators move one lane down (__shfl_sync), so after the 32nd step each
+// source is back in its lane with its sums over the warp's 64 kP targets.  Warp shuffles are
+// the second-scarcest resource here; six targets per lane keep them at 25 per 384 ordered
+// pairs for the fused sum.  The source-side sums are then added over the CTA's warps in FP64
+// (fixed order) and added into the accumulator of the source particle with a non-returning
+// atomic.
 //
 // Tile-pair schedule: particles form nt tiles of T = 64 kP WARPS.  A CTA owns one tile pair
 // (I, J), I < J.  Diagonal pair q of a launch is J - I = k (accumulator sets 4q / 4q+1 for
@@ -42,8 +43,9 @@ namespace vpm {
 
 // Build parameters: warps per CTA, resident CTAs per SM the registers are sized for (fused
 // sum VPM_ROT_MINB, three-sum operators VPM_ROT3_MINB, LES step VPM_ROT15_MINB: its 77 KB of
-// shared memory allow two; adjoint VPM_ROTG_MINB), unroll of the 32 steps, packed target
-// lanes per thread of the adjoint (VPM_ROTG_P; the others hold two).
+// shared memory allow two; adjoint VPM_ROTG_MINB / VPM_ROTGP_MINB), unroll of the 32 steps,
+// packed target lanes per thread (VPM_ROT_P, VPM_ROT3_P, VPM_ROTG_P, VPM_ROTGP_P; the LES
+// operator holds two).
 #ifndef VPM_ROT_WARPS
 #define VPM_ROT_WARPS 4
 #endif

@@ -32,16 +32,35 @@ def _field(n, seed, ring=False):
     return f
 
 
+ONE_PAST_TILE = 0  # n = one tile + 1 particle, the tile of the operator's both-sides plan
+
+
+def _one_past_tile(op, n):
+    """n, or for ONE_PAST_TILE the size whose last tile holds one particle."""
+    from openonda_b200 import kernels
+
+    if n != ONE_PAST_TILE:
+        return n
+    prev = kernels.set_symmetric_min_n(0)
+    try:
+        p = kernels.plan_info(op, "fp32c", 1 << 16, 1 << 16)
+    finally:
+        kernels.set_symmetric_min_n(prev)
+    return p["threads"] * p["targets_per_thread"] + 1
+
+
 def _dev32(f):
     return [torch.from_numpy(np.asarray(z, np.float32).astype(np.float64)).cuda()
             for z in (f.positions, f.strengths, f.radii)]
 
 
-@pytest.mark.parametrize("n,ring", [(513, False), (1000, False), (1536, False), (3001, False),
-                                    (2048, True), (4096, True), (20000, False)])
+@pytest.mark.parametrize("n,ring", [(ONE_PAST_TILE, False), (1000, False), (1536, False),
+                                    (3001, False), (2048, True), (4096, True), (20000, False)])
 @pytest.mark.parametrize("uniform_core", [False, True])
 def test_both_sides_vs_fp64(n, ring, uniform_core):
     from openonda_b200 import kernels
+
+    n = _one_past_tile("velocity_and_strength_gradients", n)
 
     f = _field(n, 7 + n, ring)
     if uniform_core:
@@ -112,14 +131,16 @@ def test_records_whole_set_and_shards(both_sides_always):
         assert normwise(joined.cpu().numpy(), ref[k].cpu().numpy()) <= tol
 
 
-@pytest.mark.parametrize("n,ring", [(513, False), (1000, False), (1536, False), (3001, False),
-                                    (2048, True), (4096, True), (20000, False)])
+@pytest.mark.parametrize("n,ring", [(ONE_PAST_TILE, False), (1000, False), (1536, False),
+                                    (3001, False), (2048, True), (4096, True), (20000, False)])
 @pytest.mark.parametrize("uniform_core", [False, True])
 @pytest.mark.parametrize("op", ["selfinduced_velocity", "strength_gradients_pse"])
 def test_velocity_and_pse_both_sides_vs_fp64(op, n, ring, uniform_core):
     """The velocity and PSE sums take the same both-sides schedule: FP32c bar against the
     FP64 one-sided sweep, and no worse than the one-sided FP32c sweep."""
     from openonda_b200 import kernels
+
+    n = _one_past_tile(op, n)
 
     f = _field(n, 5 + n, ring)
     if uniform_core:
@@ -159,14 +180,16 @@ def test_helicity_and_shards_stay_one_sided(both_sides_always):
     assert kernels.sweep_launches("strength_gradients_pse", "fp32c", n, n) > 3
 
 
-@pytest.mark.parametrize("n,ring", [(513, False), (1000, False), (3001, False), (2048, True),
-                                    (4096, True), (20000, False)])
+@pytest.mark.parametrize("n,ring", [(ONE_PAST_TILE, False), (1000, False), (3001, False),
+                                    (2048, True), (4096, True), (20000, False)])
 @pytest.mark.parametrize("uniform_core", [False, True])
 def test_les_step_sums_both_sides_vs_fp64(n, ring, uniform_core):
     """The four LES step sums (velocity, stretching, particle vorticity with the source core,
     enstrophy filter sum) on the both-sides schedule against the FP64 one-sided sweep, and
     no worse than the one-sided FP32c sweep; coincident particles add no vorticity."""
     from openonda_b200 import kernels
+
+    n = _one_past_tile("les_step_sums", n)
 
     f = _field(n, 9 + n, ring)
     if uniform_core:
@@ -197,14 +220,16 @@ def test_les_step_sums_both_sides_vs_fp64(n, ring, uniform_core):
     assert kernels.device_errors() == 0
 
 
-@pytest.mark.parametrize("n,ring", [(513, False), (1000, False), (3001, False), (2048, True),
-                                    (4096, True), (20000, False)])
+@pytest.mark.parametrize("n,ring", [(ONE_PAST_TILE, False), (1000, False), (3001, False),
+                                    (2048, True), (4096, True), (20000, False)])
 @pytest.mark.parametrize("pse", [False, True])
 def test_rhs_vjp_both_sides_vs_fp64(n, ring, pse):
     """The adjoint of (u, S [+ P]) on the both-sides schedule (each pair's derivative terms
     once for both particles) against the FP64 gather adjoint, no worse than the FP32c
     gather, and bitwise repeatable; with PSE the viscosity gradient as well."""
     from openonda_b200 import autodiff, kernels
+
+    n = _one_past_tile("rhs_vjp_pse" if pse else "rhs_vjp", n)
 
     f = _field(n, 13 + n, ring)
     x, a, s = _dev32(f)

@@ -97,7 +97,9 @@ def _field(kind):
 
     if kind == "ring":
         return configs.vortex_ring(16, 40, 1.0, 1.0, 0.1, nu=1e-3)  # N = 640
-    f = configs.random_cloud(700, seed=41, nu=1e-3)
+    if kind == "ring1600":  # three tiles or more for every both-sides sweep
+        return configs.vortex_ring(16, 100, 1.0, 1.0, 0.1, nu=1e-3)
+    f = configs.random_cloud(1700 if kind == "cloud1700" else 700, seed=41, nu=1e-3)
     f.strengths[:, 2] += 2e-3
     f.radii *= 4.0
     return f
@@ -249,10 +251,10 @@ GRAPH_CASES["ring_dns_cs_rk2_uniform_core"] = dict(
 # FP32c self sums on the both-sides schedule (forced on below its size threshold)
 GRAPH_CASES["les_pse_rk4_fp32c_both_sides"] = dict(
     flow_model="LES", viscous_scheme="PSE", time_integration_method="RK4",
-    time_step_size=0.005, precision="fp32c", both_sides=True)
+    time_step_size=0.005, precision="fp32c", field="cloud1700", both_sides=True)
 GRAPH_CASES["ring_dns_pse_rk4_fp32c_both_sides"] = dict(
     flow_model="DNS", viscous_scheme="PSE", time_integration_method="RK4",
-    time_step_size=0.005, precision="fp32c", field="ring", both_sides=True)
+    time_step_size=0.005, precision="fp32c", field="ring1600", both_sides=True)
 
 
 @pytest.mark.parametrize("name", sorted(GRAPH_CASES))
@@ -270,7 +272,9 @@ def test_advance_with_cuda_graph_equals_eager_loop(tmp_path, name):
     prev = kernels.set_symmetric_min_n(0 if both_sides else 1 << 40)
     try:
         if both_sides:
-            assert kernels.sweep_launches("selfinduced_velocity", "fp32c", f.n, f.n) > 3
+            for op in ("selfinduced_velocity", "velocity_and_strength_gradients",
+                       "strength_gradients_pse", "les_step_sums"):
+                assert kernels.sweep_launches(op, "fp32c", f.n, f.n) > 3, op
         _advance_vs_eager(tmp_path, name, cfg, f)
     finally:
         kernels.set_symmetric_min_n(prev)
