@@ -31,7 +31,8 @@ sys.path.insert(0, HERE)
 
 METRIC = "Biot-Savart Gpairs/s at N=1M: FP32-compensated vs FP64 at <=1e-6 rel err"
 UNIT = "Gpairs/s"
-# FP32-pipe work per ordered pair of the fused velocity + stretching sweep.
+# FP32-pipe work per ordered pair of the fused velocity + stretching sweep, counted from the
+# pair operators (OpVelStretch in csrc/vpm_pairs.cuh, OpVelStretchBoth in csrc/vpm_rot.cuh).
 # One-sided: 38 FP32 lane-ops = 19 FFMA + 12 FMUL + 7 FADD -> 57 flops (FMA = 2), 1 MUFU.RSQ.
 # Both-sides (each unordered pair once for both particles): 53 lane-ops = 31 FFMA + 15 FMUL
 # + 7 FADD -> 84 flops and 1 MUFU per unordered pair, i.e. 26.5 lane-ops, 42 flops and 0.5
