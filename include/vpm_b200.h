@@ -150,11 +150,12 @@ int vpm_velocity_and_strength_gradients(const double* positions, const double* s
                                         double* dalpha_dt, int precision, void* workspace,
                                         size_t workspace_bytes, void* stream);
 
-/* FP32-compensated self sums of velocity + stretching, velocity alone and PSE
- * (vpm_velocity_and_strength_gradients, vpm_selfinduced_velocity,
- * vpm_strength_gradients_pse, and vpm_sweep_records over all records) with n >= this value
- * evaluate each unordered pair once for both particles (deterministic tile-pair schedule,
- * about n / 1024 / m launches with m diagonal pairs per launch).  Sets the threshold and
+/* FP32-compensated self sums of velocity + stretching, velocity alone, PSE and the LES step
+ * sums, and the adjoint of (u, S [+ P]) (vpm_velocity_and_strength_gradients,
+ * vpm_selfinduced_velocity, vpm_strength_gradients_pse, vpm_les_step_sums, vpm_rhs_vjp, and
+ * vpm_sweep_records over all records) with n >= this value evaluate each unordered pair once
+ * for both particles (deterministic tile-pair schedule, about n / (2 T m) launches for tiles
+ * of T = 512 or 768 particles and m diagonal pairs per launch).  Sets the threshold and
  * returns the previous one (default 65536).  No counterpart in the reference. */
 int64_t vpm_set_symmetric_min_n(int64_t n);
 /* Kernel launches of one sweep of `op` (sweep and finalize, not the packing of the inputs)

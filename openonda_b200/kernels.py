@@ -231,9 +231,9 @@ def total_enstrophy(positions, strengths, radii, ref_extra_4pi=True,
 
 
 def set_symmetric_min_n(n: int) -> int:
-    """Particle count from which the FP32-compensated self sums of velocity + stretching,
-    velocity and PSE evaluate each unordered pair once for both particles; returns the
-    previous value."""
+    """Particle count from which the FP32-compensated self sums (velocity + stretching,
+    velocity, PSE, the LES step sums) and the adjoint of (u, S [+ P]) evaluate each unordered
+    pair once for both particles; returns the previous value."""
     return int(_lib.load().vpm_set_symmetric_min_n(int(n)))
 
 
