@@ -88,6 +88,7 @@ struct Plan {
   int r = 0;
   int nv = 0;
   int pairs = 0;  // both-sides sweep (vpm_rot.cuh): diagonal pairs per launch; 0 = one-sided
+  int variant = 0;  // both-sides fused sum: 0 = built for VPM_ROT_MINB CTAs/SM, 1 = _ALT
 };
 
 // FP32 self sums of velocity + stretching with at least this many particles evaluate each
@@ -422,7 +423,8 @@ struct RotSweep {
     return VPM_OK;
   }
 
-  static int plan(int64_t n, Plan* p, size_t max_partial_bytes) {
+  // eff_out: the fraction of whole waves the chosen launches fill
+  static int plan(int64_t n, Plan* p, size_t max_partial_bytes, double* eff_out = nullptr) {
     DevInfo d;
     int rc = device_info(&d);
     if (rc) return rc;
@@ -446,6 +448,7 @@ struct RotSweep {
       }
       if (eff >= 0.97) break;
     }
+    if (eff_out) *eff_out = best;
     p->pairs = best_m;
     p->tblocks = nt;
     p->splits = 4 * best_m;
@@ -583,6 +586,7 @@ struct Ops {
   using VelStretch = OpVelStretch<T, REFINE, UC>;
   using LesStep = OpLesStep<T, REFINE, UC>;
   using VelStretchBoth = OpVelStretchBoth<REFINE, UC>;  // FP32 only
+  using VelStretchBothAlt = OpVelStretchBoth<REFINE, UC, VPM_ROT_MINB_ALT>;
   using VelBoth = OpVelBoth<REFINE, UC>;                // FP32 only
   using PseBoth = OpPseBoth<REFINE, UC>;                // FP32 only
   using LesStepBoth = OpLesStepBoth<REFINE, UC>;        // FP32 only
@@ -625,8 +629,23 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
       return Sweep<typename O::Ens, T>::plan(m, n, p, mpb);
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
       if constexpr (LaneTraits<T>::kLanes == 2) {
-        if (RotSweep<typename O::VelStretchBoth>::usable(m, n, mpb))
-          return RotSweep<typename O::VelStretchBoth>::plan(n, p, mpb);
+        if (RotSweep<typename O::VelStretchBoth>::usable(m, n, mpb)) {
+          // two builds of the fused sum (3 and 2 resident CTAs per SM, the same tiles): take
+          // the one whose launches fill the waves better, the 2-CTA build on a tie (it
+          // measured equal or faster whenever its waves were as full)
+          Plan pa, pb;
+          double ea = 0.0, eb = 0.0;
+          int rc = RotSweep<typename O::VelStretchBoth>::plan(n, &pa, mpb, &ea);
+          if (!rc) rc = RotSweep<typename O::VelStretchBothAlt>::plan(n, &pb, mpb, &eb);
+          if (rc) return rc;
+          if (eb >= ea - 0.01) {
+            pb.variant = 1;
+            *p = pb;
+          } else {
+            *p = pa;
+          }
+          return VPM_OK;
+        }
       }
       return Sweep<typename O::VelStretch, T>::plan(m, n, p, mpb);
     case VPM_OP_LES_STEP_SUMS:
@@ -789,7 +808,9 @@ int run(const Call& c) {
       return rc;
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
       if constexpr (LaneTraits<T>::kLanes == 2) {
-        if (p.pairs)  // m == n: the targets are all the records (tgt_begin == 0)
+        if (p.pairs && p.variant)  // m == n: the targets are all the records (tgt_begin == 0)
+          rc = RotSweep<typename O::VelStretchBothAlt>::launch(p, src, c.n, part, c.st);
+        else if (p.pairs)
           rc = RotSweep<typename O::VelStretchBoth>::launch(p, src, c.n, part, c.st);
         else
           rc = Sweep<typename O::VelStretch, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n,

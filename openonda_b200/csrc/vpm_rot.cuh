@@ -52,6 +52,9 @@ namespace vpm {
 #ifndef VPM_ROT_MINB
 #define VPM_ROT_MINB 3
 #endif
+#ifndef VPM_ROT_MINB_ALT
+#define VPM_ROT_MINB_ALT 2
+#endif
 #ifndef VPM_ROT3_MINB
 #define VPM_ROT3_MINB 3
 #endif
@@ -165,13 +168,14 @@ struct RotStd {
   __device__ __forceinline__ static constexpr bool carried(int) { return true; }
 };
 
-// Fused velocity + stretching, both sides of the pair (FP32x2 lanes).
-template <bool REFINE, bool UC>
+// Fused velocity + stretching, both sides of the pair (FP32x2 lanes).  Built for 3 and for 2
+// resident CTAs per SM (MINB); the planner takes the one whose launches fill the waves better.
+template <bool REFINE, bool UC, int MINB = VPM_ROT_MINB>
 struct OpVelStretchBoth : RotStd<OpVelStretch<float2, REFINE, UC>, UC> {
   using V = float2;
   static constexpr int NV = 9;
   static constexpr int kP = VPM_ROT_P;
-  static constexpr int kMinBlocks = VPM_ROT_MINB;
+  static constexpr int kMinBlocks = MINB;
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
