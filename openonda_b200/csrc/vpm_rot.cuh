@@ -41,11 +41,11 @@
 
 namespace vpm {
 
-// Build parameters: warps per CTA, resident CTAs per SM the registers are sized for (fused
-// sum VPM_ROT_MINB, three-sum operators VPM_ROT3_MINB, LES step VPM_ROT15_MINB: its 77 KB of
-// shared memory allow two; adjoint VPM_ROTG_MINB / VPM_ROTGP_MINB), unroll of the 32 steps,
-// packed target lanes per thread (VPM_ROT_P, VPM_ROT3_P, VPM_ROTG_P, VPM_ROTGP_P; the LES
-// operator holds two).
+// Build parameters: warps per CTA; resident CTAs per SM the registers are sized for (fused
+// sum VPM_ROT_MINB and a second build VPM_ROT_MINB_ALT, three-sum operators VPM_ROT3_MINB,
+// LES step VPM_ROT15_MINB, whose 77 KB of shared memory allow two, adjoint VPM_ROTG_MINB and
+// VPM_ROTGP_MINB); unroll of the 32 steps; packed target lanes per thread (VPM_ROT_P,
+// VPM_ROT3_P, VPM_ROTG_P, VPM_ROTGP_P; the LES operator holds two).
 #ifndef VPM_ROT_WARPS
 #define VPM_ROT_WARPS 4
 #endif
