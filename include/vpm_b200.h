@@ -76,8 +76,13 @@ int vpm_abi_version(void);
 const char* vpm_last_error(void);
 /* Check that the current device is sm_100 (B200); VPM_ERR_ARCH otherwise. */
 int vpm_check_device(void);
-/* Read (and optionally clear) the device error word: bit 0 = a bounded wait timed out,
- * bit 1 = VPM_UNIFORM_CORE was passed for radii that are not all equal. */
+/* The compute capability the library's kernels were compiled for on the current device
+ * (cudaFuncGetAttributes binaryVersion / ptxVersion, e.g. 100 for sm_100a). */
+int vpm_binary_info(int* binary_version, int* ptx_version);
+/* Read (and optionally clear) the device error word: bit 0 = a bounded wait timed out (the
+ * sweep that gave up wrote no partial sums, so that call's outputs are not valid), bit 1 =
+ * VPM_UNIFORM_CORE was passed for radii that are not all equal.  The word is sticky until
+ * cleared. */
 int vpm_device_errors(int* out, int clear);
 /* Failure-detection self-test: one block waits on an mbarrier phase that never completes; the
  * bounded wait gives up after ~1 s, sets bit 0 of the device error word, writes 1 to the
@@ -288,18 +293,16 @@ int vpm_lattice_cylindrical(double particle_distance, double radius, double heig
  * owns the GPU's memory through its own pool.  No counterpart in the reference.  It takes no
  * workspace and calls no allocator: its scratch is a static 8 MiB device array inside the
  * library (reserved on every GPU that loads it), so n <= VPM_NOALLOC_MAX_N (larger n returns
- * VPM_ERR_ARG).  All calls share that array: calls that overlap on the GPU race.  The first
- * call on a device looks up the array's address; make it before any stream capture. */
+ * VPM_ERR_ARG).  All calls share that array: calls that overlap on the GPU race.  The array
+ * has one address per CUDA context; the first call in a context (per device) looks that
+ * address up, so make it before any stream capture.  If a sweep's bounded wait gives up
+ * (bit 0 of the vpm_device_errors word), the output is built from the previous call's
+ * partial sums: check the device error word where that matters. */
 int vpm_selfinduced_velocity_noalloc(const double* positions, const double* strengths,
                                      const double* radii, int64_t n, double* velocities,
                                      int precision, void* stream);
 
 /* ---- measurement helpers -------------------------------------------------------------- */
-/* The reference's GPU algorithm restated for comparison (ParticlesPhysicsCuda.py:133-191 when
- * which = 0, :375-445 when which = 1): one thread per target, 512 threads per block, sources
- * read from global memory, FP64 powers.  bench.py times it as the reference-algorithm GPU bar. */
-int vpm_naive_reference_kernel(int which, const double* positions, const double* strengths,
-                               const double* radii, int64_t n, double* out, void* stream);
 /* Pipe throughput kernels: blocks x threads threads each run `iters` iterations of 16
  * independent chains; one value per thread lands in `sink` (blocks*threads floats, or doubles
  * for FP64).  fp64 = 0: FP32 FMA, 1: FP64 FMA, 2: FP32 MUFU rsqrt (SFU), 3: packed FP32x2

@@ -48,6 +48,7 @@ SIGNATURES = {
     "vpm_abi_version": ([], _I),
     "vpm_last_error": ([], ctypes.c_char_p),
     "vpm_check_device": ([], _I),
+    "vpm_binary_info": ([ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
     "vpm_device_errors": ([ctypes.POINTER(_I), _I], _I),
     "vpm_selftest_bounded_wait": ([_P, _P], _I),
     "vpm_workspace_bytes": ([_I, _I, _I64, _I64], _SZ),
@@ -86,7 +87,6 @@ SIGNATURES = {
     "vpm_lattice_hexagonal": ([_P, _D, _P, _P, _I64, ctypes.POINTER(_I64), _P], _I),
     "vpm_lattice_cylindrical": ([_D, _D, _D, _P, _I, _P, _P, _I64, ctypes.POINTER(_I64), _P],
                                 _I),
-    "vpm_naive_reference_kernel": ([_I, _P, _P, _P, _I64, _P, _P], _I),
     "vpm_launch_fma_peak": ([_I, _I, _I, _I, _P, _P], _I),
 }
 

@@ -133,8 +133,13 @@ def trajectory(x0, a0, sigma, nu=None, dt=0.01, steps=10, precision="fp64",
     """Integrate ``steps`` RK4 steps; differentiable w.r.t. x0, a0, sigma (and nu).
 
     With autograd active, every segment of ``checkpoint_every`` steps is recomputed in the
-    backward pass (only segment-start states are stored).  sigma is frozen along the
-    trajectory, so equal cores (checked once) select the uniform-core forward sums."""
+    backward pass (only segment-start states are stored); ``checkpoint_every`` 0 or None
+    keeps every intermediate state instead.  sigma is frozen along the trajectory, so equal
+    cores (checked once) select the uniform-core forward sums."""
+    if checkpoint_every is not None and checkpoint_every < 0:
+        raise ValueError(f"checkpoint_every must be >= 0 or None, got {checkpoint_every}")
+    if steps < 0:
+        raise ValueError(f"steps must be >= 0, got {steps}")
     x, a = x0, a0
     with torch.no_grad():
         uc = sigma.numel() > 0 and bool((sigma == sigma.reshape(-1)[0]).all())
@@ -146,7 +151,7 @@ def trajectory(x0, a0, sigma, nu=None, dt=0.01, steps=10, precision="fp64",
 
     done = 0
     while done < steps:
-        k = min(checkpoint_every, steps - done)
+        k = min(checkpoint_every or steps, steps - done)
         if torch.is_grad_enabled() and checkpoint_every and (x.requires_grad or a.requires_grad
                                                              or sigma.requires_grad):
             x, a = checkpoint(segment, x, a, sigma, nu, k, use_reentrant=False)

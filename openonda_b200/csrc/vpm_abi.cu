@@ -1,6 +1,6 @@
 // vpm_abi.cu -- C-ABI entry points, launch planning, pack and finalize kernels.  The
-// library is one translation unit: the step, reference-algorithm and initial-condition
-// kernels are included at the end.
+// library is one translation unit: the step and initial-condition kernels are included at
+// the end.
 //
 // One pair-sum call = pack (reference AoS float64 -> packed records in the compute
 // precision, inside the caller's workspace) -> tiled sweep (partials per source split,
@@ -16,6 +16,8 @@
 #include <string>
 #include <unordered_map>
 #include <utility>
+
+#include <cuda.h>  // CUcontext / CUresult types only; no libcuda link
 
 #include "vpm_b200.h"
 #include "vpm_sweep.cuh"
@@ -1019,7 +1021,10 @@ constexpr size_t kNoAllocRecordBytes = size_t(kNoAllocMaxN) * 64;  // packed rec
 static_assert(kNoAllocRecordBytes % kAlign == 0, "record region stays 256-byte aligned");
 static_assert(kNoAllocScratchBytes > kNoAllocRecordBytes, "room for partials");
 
-std::unordered_map<int, void*> g_noalloc_addr;  // device -> device address of the scratch
+// (device, driver context) -> device address of the scratch in that context.  A __device__
+// array has one address per context, so a host application that makes another context
+// current on the same device gets its own lookup.
+std::map<std::pair<int, void*>, void*> g_noalloc_addr;
 
 int noalloc_scratch(void** out);
 
@@ -1123,19 +1128,45 @@ __global__ void rsqrt_peak_kernel(int iters, float* sink) {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[VPM_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-// Device address of g_noalloc_scratch on the current device, looked up once per device
-// (with that device current) and cached.
+// The driver context current on the calling thread (cuCtxGetCurrent, reached through the
+// runtime's driver entry-point table so the library needs no link against libcuda).
+int current_context(void** ctx) {
+  using CtxGetCurrent = CUresult (*)(CUcontext*);
+  static CtxGetCurrent fn = nullptr;
+  static std::once_flag once;
+  static cudaError_t lookup = cudaSuccess;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    lookup = cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q);
+    if (lookup == cudaSuccess && q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrent>(p);
+  });
+  if (lookup != cudaSuccess) return cuda_fail(lookup, "cudaGetDriverEntryPoint(cuCtxGetCurrent)");
+  if (!fn) return fail(VPM_ERR_CUDA, "cuCtxGetCurrent not found in the driver");
+  CUcontext c = nullptr;
+  if (fn(&c) != CUDA_SUCCESS || !c) return fail(VPM_ERR_CUDA, "no current CUDA context");
+  *ctx = c;
+  return VPM_OK;
+}
+
+// Device address of g_noalloc_scratch in the current context, looked up once per (device,
+// context) with that context current, and cached.
 int noalloc_scratch(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  void* ctx = nullptr;
+  int rc = current_context(&ctx);
+  if (rc) return rc;
   std::lock_guard<std::mutex> lk(g_mu);
-  auto it = g_noalloc_addr.find(dev);
+  const auto key = std::make_pair(dev, ctx);
+  auto it = g_noalloc_addr.find(key);
   if (it == g_noalloc_addr.end()) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-allocation scratch)");
-    it = g_noalloc_addr.emplace(dev, p).first;
+    it = g_noalloc_addr.emplace(key, p).first;
   }
   *out = it->second;
   return VPM_OK;
@@ -1152,6 +1183,16 @@ int vpm_abi_version(void) { return VPM_ABI_VERSION; }
 const char* vpm_last_error(void) { return g_last_error.c_str(); }
 
 int vpm_check_device(void) { return check_arch(); }
+
+int vpm_binary_info(int* binary_version, int* ptx_version) {
+  if (!binary_version || !ptx_version) return fail(VPM_ERR_ARG, "null result pointer");
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(&zero_kernel));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncGetAttributes");
+  *binary_version = fa.binaryVersion;
+  *ptx_version = fa.ptxVersion;
+  return VPM_OK;
+}
 
 int vpm_device_errors(int* out, int clear) {
   int v = 0;
@@ -1381,11 +1422,13 @@ int vpm_kinetic_energy_grad(const double* positions, const double* strengths,
 
 // Self-induced velocity without any allocation: the scratch (packed records and per-split
 // partial sums) lives in the library's static device array.  Every call shares that array
-// and leaves its contents behind; nothing in it needs clearing, because each call rewrites
-// every record and partial it reads.  Calls that overlap on the GPU (two streams, two host
-// threads) race on the array.  The first call on a device looks up the array's address
-// (cudaGetSymbolAddress) and the kernels' occupancy; make that first call before any stream
-// capture.
+// and leaves its contents behind; nothing in it needs clearing, because each call that
+// completes rewrites every record and partial it reads.  A sweep whose bounded wait gives up
+// returns without writing its partials: the call's output is then built from what the
+// previous call left, and only the device error word (vpm_device_errors) shows it.  Calls
+// that overlap on the GPU (two streams, two host threads) race on the array.  The first call
+// in a context looks up the array's address there (cudaGetSymbolAddress) and the kernels'
+// occupancy; make that first call before any stream capture.
 int vpm_selfinduced_velocity_noalloc(const double* positions, const double* strengths,
                                      const double* radii, int64_t n, double* velocities,
                                      int precision, void* stream) {
@@ -1441,9 +1484,6 @@ int vpm_launch_fma_peak(int fp64, int blocks, int threads, int iters, void* sink
 
 // Element-wise time-step kernels and O(N) diagnostics (same translation unit).
 #include "vpm_step.cuh"
-
-// The reference's GPU algorithm restated (measurement only).
-#include "vpm_naive.cuh"
 
 // Initial conditions and particle lattices on the device.
 #include "vpm_ic.cuh"

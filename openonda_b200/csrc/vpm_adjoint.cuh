@@ -110,6 +110,7 @@ template <class V, bool REFINE, bool PSE>
 struct OpRhsVjp {
   static constexpr int NV = PSE ? 18 : 14;
   static constexpr int kR = 2;  // register-heavy: one FP32 lane (two targets) per thread
+  static constexpr int kWindow = 0;  // the sweep's default FP32 window
   using Record = RecG<V>;
   using SrcT = SrcG<V>;
   using TgtT = TgtG<V>;

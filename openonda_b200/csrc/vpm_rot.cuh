@@ -32,8 +32,9 @@
 // order.
 //
 // Accumulation: target side in FP32 per batch of 32 sources, folded into FP64 carries held in
-// shared memory; source side in FP32 over the warp's 64 kP targets (each half of the packed
-// accumulator sums 32 kP terms), then FP64 across warps and tile pairs.
+// shared memory; source side in FP32 over windows of kSrcWindow steps (each half of the
+// packed accumulator sums kSrcWindow kP terms), the windows of a batch added in FP32 in
+// shared memory, then both halves in FP64 across warps and tile pairs.
 #pragma once
 
 #include "vpm_adjoint.cuh"
@@ -110,9 +111,27 @@ __host__ __device__ constexpr int rot_tile() {
   return 64 * Op::kP * kRotWarps;
 }
 
+// Source-side window (Op::kSrcWindow steps): at the end of a window each lane adds the packed
+// FP32 sums of the source it holds into that source's slot in shared memory and starts again
+// from zero, so no FP32 sum runs over more than kSrcWindow * kP terms.  The stretching sums
+// (fused, LES step) take short windows for accuracy; velocity, PSE and the adjoint, whose
+// errors are far inside their bars, take one window per batch.
+#ifndef VPM_ROT_SRC_WINDOW
+#define VPM_ROT_SRC_WINDOW 8
+#endif
+#ifndef VPM_ROT3_SRC_WINDOW
+#define VPM_ROT3_SRC_WINDOW 32
+#endif
+#ifndef VPM_ROTG_SRC_WINDOW
+#define VPM_ROTG_SRC_WINDOW 32
+#endif
+#ifndef VPM_ROT_TGT_WINDOW
+#define VPM_ROT_TGT_WINDOW 32
+#endif
+
 constexpr size_t rot_smem_bytes(int nv, int tile) {
-  return size_t(tile) * nv * sizeof(double) +               // target-side FP64 carries
-         size_t(2) * kRotWarps * 32 * nv * sizeof(float);  // source-side sums, double-buffered
+  return size_t(tile) * nv * sizeof(double) +                // target-side FP64 carries
+         size_t(2) * kRotWarps * 32 * nv * sizeof(float2);  // source-side sums, double-buffered
 }
 
 // The source a lane holds on the standard 64-byte record: position, core, strength.
@@ -177,6 +196,8 @@ struct OpVelStretchBoth : RotStd<OpVelStretch<float2, REFINE, UC>, UC> {
   static constexpr int kP = VPM_ROT_P;
   static constexpr int kMinBlocks = MINB;
   static constexpr int kUnroll = VPM_ROT_UNROLL;
+  static constexpr int kSrcWindow = VPM_ROT_SRC_WINDOW;
+  static constexpr int kTgtWindow = VPM_ROT_TGT_WINDOW;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -227,6 +248,8 @@ struct OpVelBoth : RotStd<OpVel<float2, REFINE, UC>, UC> {
   static constexpr int kP = VPM_ROT3_P;
   static constexpr int kMinBlocks = VPM_ROT3_MINB;
   static constexpr int kUnroll = VPM_ROT_UNROLL;
+  static constexpr int kSrcWindow = VPM_ROT3_SRC_WINDOW;
+  static constexpr int kTgtWindow = 32;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -263,6 +286,8 @@ struct OpPseBoth : RotStd<OpPse<float2, REFINE, UC>, UC> {
   static constexpr int kP = VPM_ROT3_P;
   static constexpr int kMinBlocks = VPM_ROT3_MINB;
   static constexpr int kUnroll = VPM_ROT_UNROLL;
+  static constexpr int kSrcWindow = VPM_ROT3_SRC_WINDOW;
+  static constexpr int kTgtWindow = 32;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -300,6 +325,8 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
   static constexpr int NV = 15;
   static constexpr int kMinBlocks = VPM_ROT15_MINB;
   static constexpr int kUnroll = VPM_ROT15_UNROLL;
+  static constexpr int kSrcWindow = VPM_ROT_SRC_WINDOW;
+  static constexpr int kTgtWindow = VPM_ROT_TGT_WINDOW;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -408,6 +435,8 @@ struct OpRhsVjpBoth {
   static constexpr int kP = PSE ? VPM_ROTGP_P : VPM_ROTG_P;
   static constexpr int kMinBlocks = PSE ? VPM_ROTGP_MINB : VPM_ROTG_MINB;
   static constexpr int kUnroll = PSE ? VPM_ROTGP_UNROLL : VPM_ROTG_UNROLL;
+  static constexpr int kSrcWindow = VPM_ROTG_SRC_WINDOW;
+  static constexpr int kTgtWindow = 32;
 
   __device__ __forceinline__ static Lane load_lane(const Record* rec, int64_t j, int64_t n) {
     if (j < n) {
@@ -561,9 +590,15 @@ rot_sweep_kernel(const RotArgs a) {
   constexpr int NV = Op::NV;
   constexpr int P = Op::kP;
   constexpr int T = rot_tile<Op>();
+  constexpr int WT = kRotWarps * 32;  // source slots of a batch: [warp][source lane]
+  constexpr int SW = Op::kSrcWindow;
+  constexpr int TW = Op::kTgtWindow;
+  static_assert(32 % SW == 0, "the source window divides the 32 steps of a batch");
+  static_assert(32 % TW == 0 && TW % SW == 0, "target windows are whole source windows");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* car = reinterpret_cast<double*>(smem_raw);  // [NV][T]
-  float* jbuf = reinterpret_cast<float*>(smem_raw + size_t(T) * NV * sizeof(double));
+  // [2][NV][WT]: each warp's packed source-side sums of the current batch, per source
+  float2* jbuf = reinterpret_cast<float2*>(smem_raw + size_t(T) * NV * sizeof(double));
   const Record* rec = static_cast<const Record*>(a.rec);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -620,55 +655,79 @@ rot_sweep_kernel(const RotArgs a) {
     float2 jv[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) jv[v] = make_float2(0.f, 0.f);
+    float2* jb = jbuf + (b & 1) * (NV * WT);
     const int src_lane = (lane + 1) & 31;
+    for (int w = 0; w < 32 / SW; ++w) {
 #pragma unroll Op::kUnroll
-    for (int step = 0; step < 32; ++step) {
-      const typename Op::SrcT src = Op::broadcast(cur);
+      for (int st = 0; st < SW; ++st) {
+        const int step = w * SW + st;
+        const typename Op::SrcT src = Op::broadcast(cur);
 #pragma unroll
-      for (int p = 0; p < P; ++p) {
-        if constexpr (DIAG) {
-          // at this step the lane holds source b * 32 + ((lane + step) mod 32) of the tile
-          const int64_t ti[2] = {i0 + lt[2 * p], i0 + lt[2 * p + 1]};
-          Op::diag(tg[p], acc[p], src, ti, j0 + b * 32 + ((lane + step) & 31));
-        } else {
-          Op::pair2(tg[p], acc[p], jv, src);
+        for (int p = 0; p < P; ++p) {
+          if constexpr (DIAG) {
+            // at this step the lane holds source b * 32 + ((lane + step) mod 32) of the tile
+            const int64_t ti[2] = {i0 + lt[2 * p], i0 + lt[2 * p + 1]};
+            Op::diag(tg[p], acc[p], src, ti, j0 + b * 32 + ((lane + step) & 31));
+          } else {
+            Op::pair2(tg[p], acc[p], jv, src);
+          }
+        }
+        // pass the source one lane down (lane l now holds what lane l+1 held); its sums move
+        // with it, except after a window's last step, where they are stored instead
+        Op::shuffle(cur, src_lane);
+        if constexpr (!DIAG) {
+          if (st != SW - 1) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+              if (Op::carried(v)) {
+                jv[v].x = __shfl_sync(0xffffffffu, jv[v].x, src_lane);
+                jv[v].y = __shfl_sync(0xffffffffu, jv[v].y, src_lane);
+              }
+            }
+          }
         }
       }
-      // pass the source (and its sums) one lane down: lane l now holds what lane l+1 held
-      Op::shuffle(cur, src_lane);
       if constexpr (!DIAG) {
+        // end of a window: the lane holds the sums of the source it met at the window's last
+        // step, (lane + step) mod 32; add them into that source's slot (the lanes of a warp
+        // hold distinct sources) and start the next window from zero
+        const int slot = warp * 32 + ((lane + (w + 1) * SW - 1) & 31);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           if (Op::carried(v)) {
-            jv[v].x = __shfl_sync(0xffffffffu, jv[v].x, src_lane);
-            jv[v].y = __shfl_sync(0xffffffffu, jv[v].y, src_lane);
+            float2* e = jb + v * WT + slot;
+            *e = (w == 0) ? jv[v] : (*e + jv[v]);
+            jv[v] = make_float2(0.f, 0.f);
+          }
+        }
+      }
+      if (((w + 1) * SW) % TW == 0) {
+        // target side: the window's FP32 sums into the FP64 carries (each thread its own rows)
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) {
+            car[v * T + lt[2 * p]] += double(acc[p][v].x);
+            car[v * T + lt[2 * p + 1]] += double(acc[p][v].y);
+            acc[p][v] = make_float2(0.f, 0.f);
           }
         }
       }
     }
-    // target side: this batch's FP32 sums into the FP64 carries (each thread its own rows)
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        car[v * T + lt[2 * p]] += double(acc[p][v].x);
-        car[v * T + lt[2 * p + 1]] += double(acc[p][v].y);
-        acc[p][v] = make_float2(0.f, 0.f);
-      }
-    }
     if constexpr (!DIAG) {
-      // after 32 steps lane l holds the sums of source b*32 + l again
-      float* jb = jbuf + (b & 1) * (kRotWarps * 32 * NV);
-#pragma unroll
-      for (int v = 0; v < NV; ++v) jb[(warp * 32 + lane) * NV + v] = jv[v].x + jv[v].y;
       __syncthreads();  // one barrier per batch; jbuf is double-buffered
       const int nsrc = (cnt - b * 32 < 32) ? cnt - b * 32 : 32;
-      for (int q = tid; q < nsrc * NV; q += kRotThreads) {
-        const int jj = q / NV, v = q - jj * NV;
-        if (!Op::carried(v)) continue;
+      for (int q = tid; q < 32 * NV; q += kRotThreads) {
+        const int v = q >> 5, jj = q & 31;  // consecutive threads: consecutive sources
+        if (jj >= nsrc || !Op::carried(v)) continue;
+        // both packed halves of every warp's sum, in FP64, in a fixed order
         double sum = 0.0;
 #pragma unroll
-        for (int w = 0; w < kRotWarps; ++w) sum += double(jb[(w * 32 + jj) * NV + v]);
+        for (int w = 0; w < kRotWarps; ++w) {
+          const float2 e = jb[v * WT + w * 32 + jj];
+          sum += double(e.x);
+          sum += double(e.y);
+        }
         // the only writer of this element in this launch, so the fire-and-forget reduction
         // adds in a fixed order (launch order) and the thread does not wait for the load
         atomicAdd(&a.acc[(int64_t(set_j) * NV + v) * a.n + (j0 + b * 32 + jj)], -sum);

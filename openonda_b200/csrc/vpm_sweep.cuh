@@ -7,9 +7,10 @@
 // completion is signalled on an mbarrier, and all warps read the tile by broadcast.
 //
 // Accumulation: in FP64 the partial sums accumulate directly in double.  In FP32 each
-// target keeps an FP32 accumulator for a window of CW=32 consecutive sources and folds
-// it into an FP64 carry at the end of every window (one DADD per value per 32 pairs), so
-// rounding grows only over 32 terms and the long sum over N sources runs in FP64.  FP32
+// target keeps an FP32 accumulator for a window of CW consecutive sources (32; 16 for the
+// stretching operators) and folds it into an FP64 carry at the end of every window (one DADD
+// per value per window), so rounding grows only over CW terms and the long sum over N
+// sources runs in FP64.  FP32
 // targets are processed two at a time with the paired FP32 instructions of sm_100.
 //
 // Each (split, value, target) partial is written as FP64 to
@@ -63,6 +64,8 @@ sweep_kernel(const SweepArgs<typename Op::Record> a) {
   constexpr int L = LaneTraits<V>::kLanes;
   constexpr int P = R / L;
   constexpr bool kCarry = (L == 2);
+  constexpr int CW = Op::kWindow ? Op::kWindow : kCarryWindow;  // sources per FP32 window
+  static_assert(kCarryWindow % CW == 0, "windows tile the sweep's source chunks");
   constexpr bool kSmemCarry = kCarry && VPM_SMEM_CARRY;
   constexpr uint32_t kRecBytes = sizeof(RecT);
   static_assert(R % L == 0, "targets per thread must fill whole lanes");
@@ -138,8 +141,8 @@ sweep_kernel(const SweepArgs<typename Op::Record> a) {
     const int64_t left = count - static_cast<int64_t>(t) * TILE;
     const int cnt = static_cast<int>(left < TILE ? left : TILE);
     if (ok) {
-      for (int w = 0; w < cnt; w += kCarryWindow) {
-        const int e = (w + kCarryWindow < cnt) ? w + kCarryWindow : cnt;
+      for (int w = 0; w < cnt; w += CW) {
+        const int e = (w + CW < cnt) ? w + CW : cnt;
 #pragma unroll kSrcUnroll
         for (int j = w; j < e; ++j) {
           const typename Op::SrcT src = Op::load(tile[j]);

@@ -2,9 +2,10 @@
 
 Each rank owns a contiguous shard of the particles.  One sweep is:
 
-1. pack the rank's own shard into compute-precision records (32 B each in FP32),
+1. pack the rank's own shard into compute-precision records (64 B each in both precisions:
+   FP64 values, or FP32 values stored twice for the paired FP32 instructions),
 2. all-gather the records of every shard (NCCL over NVLink; the only exchange step of the
-   all-pairs sum -- 32 MB at N = 2^20),
+   all-pairs sum -- 64 MB at N = 2^20),
 3. sweep the rank's own targets against all gathered sources with ``vpm_sweep_records``.
 
 Targets are independent, so nothing else crosses GPUs; the outputs stay sharded.  The

@@ -541,6 +541,9 @@ class ParticleSystem:
                                 d["Viscosity"], d["Viscosity_t"], d["Group_ID"])
         self.time_step = int(d["time_step"])
         self.flow_time = float(d["flow_time"])
+        if "time_step_size" in d.files:
+            # the BDF history and the flow time were built with this step size
+            self.time_step_size = float(d["time_step_size"])
         if "history_1" in d.files:
             self._hist = [self._as_dev(d[f"history_{k}"]) for k in (1, 2, 3)]
         self._les = self._as_dev(d["les_state"])

@@ -98,6 +98,24 @@ def test_trajectory_gradient_vs_dense_autograd():
         assert normwise(g[k].cpu().numpy(), ref[k].numpy()) <= 1e-10, k
 
 
+@pytest.mark.parametrize("every", [0, None])
+def test_trajectory_without_checkpointing_matches_checkpointed(every):
+    """checkpoint_every 0 or None keeps every state (no recompute) and gives the same
+    gradient as segment checkpointing."""
+    from openonda_b200 import autodiff
+
+    x, a, s, _ = _field(256, 22, scale=8.0)
+    dt, steps = 0.01, 3
+    grads = []
+    for ck in (every, 2):
+        cx, ca, cs = [z.requires_grad_() for z in _cuda(x, a, s)]
+        xT, aT = autodiff.trajectory(cx, ca, cs, None, dt, steps, "fp64", checkpoint_every=ck)
+        e = autodiff.kinetic_energy(xT, aT, cs, "fp64")
+        grads.append(torch.autograd.grad(e, (cx, ca, cs)))
+    for u, v in zip(*grads):
+        assert torch.equal(u, v)
+
+
 def test_trajectory_gradient_vs_central_differences():
     from openonda_b200 import autodiff, configs
 

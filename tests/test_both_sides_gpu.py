@@ -12,6 +12,15 @@ from conftest import normwise
 
 pytestmark = pytest.mark.gpu
 
+# Stretching on the coarse test rings (2048 and 4096 particles, a few particles per core
+# width) is a residual of strongly cancelling near-neighbour terms: both sweeps lose more
+# digits there (measured 6e-6 to 1.3e-5) than on the benchmark rings (<= 2e-6).
+COARSE_RING_STRETCH_TOL = 1.5e-5
+
+
+def _stretch_tol(ring, e_one):
+    return COARSE_RING_STRETCH_TOL if ring else max(2e-6, 1.5 * e_one)
+
 
 @pytest.fixture
 def both_sides_always():
@@ -82,9 +91,9 @@ def test_both_sides_vs_fp64(n, ring, uniform_core):
         e_both = normwise(both[k].cpu().numpy(), ref[k].cpu().numpy())
         e_one = normwise(one32[k].cpu().numpy(), ref[k].cpu().numpy())
         print(f"n={n} ring={ring} uc={uniform_core} k={k}: both {e_both:.2e} one {e_one:.2e}")
-        # velocity: the FP32c bar; stretching: no worse than the one-sided FP32c sweep
-        # (on these coarse rings both exceed the ring-8192 figure)
-        assert e_both <= (1e-6 if k == 0 else max(5e-6, 1.5 * e_one)), (k, e_both, e_one)
+        # velocity: the FP32c bar; stretching: the stretching bar on random clouds (or no
+        # worse than the one-sided sweep), COARSE_RING_STRETCH_TOL on the coarse rings
+        assert e_both <= (1e-6 if k == 0 else _stretch_tol(ring, e_one)), (k, e_both, e_one)
     assert kernels.device_errors() == 0
 
 
@@ -125,7 +134,7 @@ def test_records_whole_set_and_shards(both_sides_always):
 
     full = sweep(0, n)
     parts = [sweep(0, 1000), sweep(1000, 1200), sweep(2200, 800)]
-    for k, tol in ((0, 1e-6), (1, 5e-6)):
+    for k, tol in ((0, 1e-6), (1, 2e-6)):
         joined = torch.cat([p[k] for p in parts])
         assert normwise(full[k].cpu().numpy(), ref[k].cpu().numpy()) <= tol
         assert normwise(joined.cpu().numpy(), ref[k].cpu().numpy()) <= tol
@@ -213,7 +222,7 @@ def test_les_step_sums_both_sides_vs_fp64(n, ring, uniform_core):
         e_one = normwise(one32[k].cpu().numpy(), ref[k].cpu().numpy())
         print(f"les n={n} ring={ring} uc={uniform_core} k={k}: both {e_both:.2e} "
               f"one {e_one:.2e}")
-        assert e_both <= (1e-6 if k != 1 else max(5e-6, 1.5 * e_one)), (k, e_both, e_one)
+        assert e_both <= (1e-6 if k != 1 else _stretch_tol(ring, e_one)), (k, e_both, e_one)
         assert torch.equal(both[k], again[k])
     e_ref, e_got = float(ref[3]), float(both[3])
     assert abs(e_got - e_ref) <= 1e-6 * abs(e_ref)
@@ -270,13 +279,13 @@ def test_refined_rsqrt_both_sides(both_sides_always):
     assert kernels.sweep_launches("velocity_and_strength_gradients", p, n, n) > 3
     pairs = [
         (kernels.velocity_and_strength_gradients(x, a, s, precision=p),
-         kernels.velocity_and_strength_gradients(x, a, s, precision="fp64"), (1e-6, 5e-6)),
+         kernels.velocity_and_strength_gradients(x, a, s, precision="fp64"), (1e-6, 2e-6)),
         ((kernels.selfinduced_velocity(x, a, s, precision=p),),
          (kernels.selfinduced_velocity(x, a, s, precision="fp64"),), (1e-6,)),
         ((kernels.strength_gradients_pse(x, a, s, nu, precision=p),),
          (kernels.strength_gradients_pse(x, a, s, nu, precision="fp64"),), (1e-6,)),
         (kernels.les_step_sums(x, a, s, precision=p)[:3],
-         kernels.les_step_sums(x, a, s, precision="fp64")[:3], (1e-6, 5e-6, 1e-6)),
+         kernels.les_step_sums(x, a, s, precision="fp64")[:3], (1e-6, 2e-6, 1e-6)),
     ]
     for got, ref, tols in pairs:
         for g, r, tol in zip(got, ref, tols):

@@ -1,0 +1,202 @@
+"""The benchmark workloads at their stated sizes, on short horizons, gated.
+
+* Leapfrogging rings, N = 131072 (two coaxial rings R=1, sigma=0.08, 256 x 256 each), DNS +
+  PSE + RK4 at dt = 0.005: three steps in FP32-compensated form and in FP64 from the same
+  FP32-rounded state.  After every step the FP32c sums of the FP32c state are held against
+  the FP64 sums of the same state (velocity 1e-6, stretching 2e-6), and the two trajectories
+  and their FP64 diagnostics (circulation, linear impulse) must agree.
+* Perturbed ring, N = 65536 (R=1, sigma=0.1, radial modes 2-8), loss = FP64-summed kinetic
+  energy after two RK4 steps at dt = 0.01 with a checkpoint every step: the FP32c adjoint
+  gradient against the FP64 adjoint gradient (1e-5), and the FP64 adjoint against FP64
+  central differences (h = 1e-6) on 8 coordinates.
+* Dynamic-LES ring, N = 2^20 (R=1, sigma=0.05, azimuthal noise 0.01, nu=1e-5), LES + PSE +
+  RK4 at dt = 0.002: one step in FP32c and in FP64.  The FP32c sums of the stepped state
+  against FP64 (velocity, vorticity and enstrophy 1e-6, stretching 2e-6), the dynamic
+  coefficient C_nu of the two runs, and the FP64 LES step sums of the initial state against
+  the oracle on windows of targets at the start, middle and end of the 2^20 rows.
+
+The reference's vpmModule.py step (:522-560) and strength update with the LES coefficient
+(:713-884, :887-962) are what the ParticleSystem steps restate."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import normwise
+
+pytestmark = pytest.mark.gpu
+
+VEL_TOL = 1e-6       # FP32c velocity (and vorticity, enstrophy) against FP64
+STRETCH_TOL = 2e-6   # FP32c stretching against FP64 on ring-shaped fields
+FP64_TOL_2_20 = 1e-11  # FP64 against the oracle at 2^20 sources (see test_fullsize_gpu)
+
+
+def _system(tmp_path, name, precision, **cfg):
+    from openonda_b200.vpm.vpmModule import ParticleSystem
+
+    return ParticleSystem(monitor_variables=[], backup_frequency=10 ** 9,
+                          backup_filename=str(tmp_path / name), precision=precision, **cfg)
+
+
+def _r32(z):
+    return np.asarray(z, dtype=np.float32).astype(np.float64)
+
+
+def _load(ps, f):
+    ps.add_particle_field(_r32(f.positions), np.zeros_like(f.positions), _r32(f.strengths),
+                          _r32(f.radii), _r32(f.viscosities))
+
+
+def _step(ps):
+    ps.update_velocities()
+    ps.update_strengths()
+    ps.update_state()
+
+
+def _sums_fp32c_vs_fp64(ps):
+    """Velocity and stretching of the system's state, FP32c against FP64 on the same
+    FP32-rounded inputs."""
+    from openonda_b200 import kernels
+
+    x, a, s = (t.float().double() for t in (ps.positions, ps.strengths, ps.radii))
+    u64, g64 = kernels.velocity_and_strength_gradients(x, a, s, precision="fp64")
+    u32, g32 = kernels.velocity_and_strength_gradients(x, a, s, precision="fp32c",
+                                                       uniform_core=ps._uc)
+    return (normwise(u32.cpu().numpy(), u64.cpu().numpy()),
+            normwise(g32.cpu().numpy(), g64.cpu().numpy()))
+
+
+def test_leapfrog_rings_131072_three_steps(tmp_path):
+    from openonda_b200 import configs
+
+    f = configs.leapfrog_rings()
+    assert f.n == 131072
+    cfg = dict(flow_model="DNS", viscous_scheme="PSE", time_integration_method="RK4",
+               time_step_size=0.005)
+    p32 = _system(tmp_path, "a", "fp32c", **cfg)
+    p64 = _system(tmp_path, "b", "fp64", **cfg)
+    _load(p32, f)
+    _load(p64, f)
+    for k in range(1, 4):
+        _step(p32)
+        _step(p64)
+        eu, eg = _sums_fp32c_vs_fp64(p32)
+        print(f"leapfrog step {k}: velocity {eu:.2e} stretching {eg:.2e}")
+        assert eu <= VEL_TOL and eg <= STRETCH_TOL, (k, eu, eg)
+    # the trajectories part by the FP32c sum errors times the step: far below the step itself
+    ex = normwise(p32.get_particle_positions(), p64.get_particle_positions())
+    ea = normwise(p32.get_particle_strengths(), p64.get_particle_strengths())
+    print(f"leapfrog after 3 steps: positions {ex:.2e} strengths {ea:.2e}")
+    assert ex <= 1e-8 and ea <= 1e-6
+    d32, d64 = p32._diagnostics(), p64._diagnostics()
+    assert abs(d32[0] - d64[0]) <= 1e-7 * abs(d64[0])  # total circulation (FP64 sum)
+    imp = np.linalg.norm(d64[4:7])
+    assert np.linalg.norm(d32[4:7] - d64[4:7]) <= 1e-7 * imp  # linear impulse
+    from openonda_b200 import kernels
+
+    assert kernels.device_errors() == 0
+
+
+def test_perturbed_ring_65536_trajectory_gradient():
+    from openonda_b200 import autodiff, configs
+
+    f = configs.perturbed_ring()
+    assert f.n == 65536
+    dev = torch.device("cuda")
+    x0, a0, s0 = (torch.from_numpy(_r32(z)).to(dev) for z in (f.positions, f.strengths, f.radii))
+    dt, steps, every = 0.01, 2, 1
+
+    def grad(prec):
+        x, a, s = (z.clone().requires_grad_() for z in (x0, a0, s0))
+        xT, aT = autodiff.trajectory(x, a, s, None, dt, steps, prec, checkpoint_every=every)
+        e = autodiff.kinetic_energy(xT, aT, s, prec)
+        return torch.autograd.grad(e, (x, a, s))
+
+    g32, g64 = grad("fp32c"), grad("fp64")
+    for k, name in enumerate(("positions", "strengths", "radii")):
+        e = normwise(g32[k].cpu().numpy(), g64[k].cpu().numpy())
+        print(f"gradient w.r.t. {name}: fp32c vs fp64 {e:.2e}")
+        assert e <= 1e-5, (name, e)
+
+    def loss64(x, a, s):
+        with torch.no_grad():
+            xT, aT = autodiff.trajectory(x, a, s, None, dt, steps, "fp64")
+            return float(autodiff.kinetic_energy(xT, aT, s, "fp64"))
+
+    rng = np.random.default_rng(2024)
+    h = 1e-6
+    bases = (x0, a0, s0)
+    for q in range(8):
+        which = q % 3
+        base = bases[which]
+        idx = tuple(int(rng.integers(0, d)) for d in base.shape)
+        step = h * (float(a0.abs().max()) if which == 1 else 1.0)
+        bp, bm = base.clone(), base.clone()
+        bp[idx] += step
+        bm[idx] -= step
+        args_p, args_m = list(bases), list(bases)
+        args_p[which], args_m[which] = bp, bm
+        fd = (loss64(*args_p) - loss64(*args_m)) / (2 * step)
+        scale = float(g64[which].abs().max())
+        err = abs(float(g64[which][idx]) - fd) / scale
+        print(f"FD coordinate {which}{idx}: adjoint {float(g64[which][idx]):.6e} fd {fd:.6e}")
+        assert err <= 1e-5, (which, idx, err)
+
+
+def test_les_ring_2e20_one_step(tmp_path):
+    from openonda_b200 import configs, kernels
+
+    f = configs.les_ring()
+    n = f.n
+    assert n == 1 << 20
+    cfg = dict(flow_model="LES", viscous_scheme="PSE", time_integration_method="RK4",
+               time_step_size=0.002)
+    p32 = _system(tmp_path, "a", "fp32c", **cfg)
+    p64 = _system(tmp_path, "b", "fp64", **cfg)
+    _load(p32, f)
+    _load(p64, f)
+    assert p32._uc  # one core for the whole ring: the uniform-core sweeps
+    _step(p32)
+    _step(p64)
+    eu, eg = _sums_fp32c_vs_fp64(p32)
+    print(f"LES ring after one step: velocity {eu:.2e} stretching {eg:.2e}")
+    assert eu <= VEL_TOL and eg <= STRETCH_TOL
+    x, a, s = (t.float().double() for t in (p32.positions, p32.strengths, p32.radii))
+    l64 = kernels.les_step_sums(x, a, s, precision="fp64")
+    l32 = kernels.les_step_sums(x, a, s, precision="fp32c", uniform_core=True)
+    ew = normwise(l32[2].cpu().numpy(), l64[2].cpu().numpy())
+    ee = abs(float(l32[3]) - float(l64[3])) / abs(float(l64[3]))
+    print(f"LES filter sums: vorticity {ew:.2e} enstrophy {ee:.2e}")
+    assert ew <= VEL_TOL and ee <= VEL_TOL
+    # the dynamic coefficient follows the enstrophy ratio, whose FP32c error is ~1e-8
+    c32, c64 = p32.Cnu, p64.Cnu
+    print(f"C_nu fp32c {c32!r} fp64 {c64!r}")
+    assert abs(c32 - c64) <= 1e-7 * abs(c64)
+    ex = normwise(p32.get_particle_positions(), p64.get_particle_positions())
+    ea = normwise(p32.get_particle_strengths(), p64.get_particle_strengths())
+    print(f"LES ring after one step: positions {ex:.2e} strengths {ea:.2e}")
+    assert ex <= 1e-8 and ea <= 1e-6
+    assert kernels.device_errors() == 0
+
+
+def test_les_ring_2e20_sums_vs_oracle_windows():
+    """FP64 LES step sums (velocity, stretching, particle vorticity) of the 2^20 ring against
+    the oracle on target windows across the whole range of rows."""
+    from openonda_b200 import configs, kernels
+
+    f = configs.les_ring()
+    n = f.n
+    dev = torch.device("cuda")
+    x, a, s = (torch.from_numpy(np.ascontiguousarray(z)).to(dev)
+               for z in (f.positions, f.strengths, f.radii))
+    u, g, w, _ = kernels.les_step_sums(x, a, s, precision="fp64", uniform_core=True)
+    u, g, w = u.cpu().numpy(), g.cpu().numpy(), w.cpu().numpy()
+    for t0 in (0, n // 2 - 96, n - 192):
+        t1 = t0 + 192
+        ru = oracle.gpu.selfinduced_velocity_range(f.positions, f.strengths, f.radii, t0, t1)
+        rg = oracle.gpu.strength_gradients_range(f.positions, f.strengths, f.radii, t0, t1)
+        rw = oracle.gpu.get_vorticity_field_at(f.positions[t0:t1], f.positions, f.strengths,
+                                               f.radii)
+        es = [normwise(u[t0:t1], ru), normwise(g[t0:t1], rg), normwise(w[t0:t1], rw)]
+        print(f"window [{t0}, {t1}): " + ", ".join(f"{e:.2e}" for e in es))
+        assert max(es) <= FP64_TOL_2_20, (t0, es)

@@ -16,7 +16,7 @@ FP64_TOL = 1e-12
 FP32C_TOL = 1e-6  # velocity (and PSE, vorticity, enstrophy)
 # Stretching on ring-shaped fields is a small residual of cancelling near-neighbour
 # terms, which amplifies the ulp-level FP32 pair error; its error is stated, bounded here.
-FP32C_STRETCH_TOL = 5e-6
+FP32C_STRETCH_TOL = 2e-6
 
 
 @pytest.fixture(scope="module")
@@ -266,23 +266,17 @@ def test_records_target_shards_reassemble():
         assert abs(ke - float(ke_full)) <= 1e-12 * abs(float(ke_full))
 
 
-def test_naive_reference_kernels_match_oracle():
-    """The measurement-only restatement of the reference's GPU kernels computes the same sums."""
-    import torch
+def test_loaded_kernels_are_sm100a_binaries():
+    """The kernels the runtime loaded on this device were compiled for compute capability 10.0
+    (the library embeds sm_100a code only)."""
+    import ctypes
 
-    from openonda_b200 import _lib, configs
+    from openonda_b200 import _lib
 
-    f = configs.random_cloud(1500, seed=31)
-    f.radii *= 5
-    lib = _lib.load()
-    x, a, s = (torch.from_numpy(z).cuda() for z in (f.positions, f.strengths, f.radii))
-    out = torch.empty((1500, 3), dtype=torch.float64, device="cuda")
-    st = torch.cuda.current_stream().cuda_stream
-    for which, ref in ((0, oracle.gpu.get_selfinduced_velocity),
-                       (1, oracle.gpu.get_strength_gradients)):
-        _lib.check(lib.vpm_naive_reference_kernel(which, x.data_ptr(), a.data_ptr(),
-                                                  s.data_ptr(), 1500, out.data_ptr(), st))
-        assert normwise(out.cpu().numpy(), ref(f.positions, f.strengths, f.radii)) <= 1e-13
+    b, p = ctypes.c_int(), ctypes.c_int()
+    _lib.check(_lib.load().vpm_binary_info(ctypes.byref(b), ctypes.byref(p)))
+    assert b.value == 100, b.value
+    assert _lib.load().vpm_check_device() == 0
 
 
 @pytest.mark.parametrize("n", [1, 97, 2048, 5000])

@@ -107,9 +107,10 @@ def test_checkpoint_resume_is_exact(tmp_path, use_graph):
     ck = str(tmp_path / "ck.npz")
     a.save_checkpoint(ck)
     a.advance(4, use_graph=use_graph)
-    b = _system(tmp_path / "b", **cfg)
+    # built with another step size: the checkpoint's step size must take over
+    b = _system(tmp_path / "b", **dict(cfg, time_step_size=0.02))
     b.load_checkpoint(ck)
-    assert b.time_step == 5
+    assert b.time_step == 5 and b.time_step_size == 0.005
     b.advance(4, use_graph=use_graph)
     for get in ("get_particle_positions", "get_particle_strengths", "get_particle_radii",
                 "get_particle_velocities", "get_particle_viscosities_t"):

@@ -1,6 +1,6 @@
 """The five benchmark workloads, run through the public API; one JSON line per result.
 
-    python -m openonda_b200.workloads {config1,config2,config3,config4,config5,stepkernels} [opts]
+    python workloads.py {config1,config2,config3,config4,config5,stepkernels} [opts]
 
 config1  ring N=8192 (64 x 128 torus lattice), FP64, one DNS+PSE RK4 step at dt=0.01,
          compared with the CPU oracle's restatement of the reference step.
@@ -16,6 +16,8 @@ config4  differentiation: perturbed ring N=65536, FP32c, loss = FP64-summed kine
 config5  dynamic-LES ring N=2^20, FP32c, PSE, RK4 dt=0.002: time per step, Gpairs/s, error vs
          FP64 at the last step.
 stepkernels  GB/s of the element-wise step kernels (RK stage, RK4 combine, BDF) at N=2^22.
+reference    the reference's own Numba-CUDA kernels (GPU) and Numba CPU module (host cores),
+             from baseline/_ref, on the random cloud (default N=131072).
 sweeps       time of each FP32c sweep of an LES step (fused LES sums vs the sweeps they replace).
 peaks        FP32 FFMA / FFMA2 / mixed / MUFU rsqrt throughput microbenchmarks.
 
@@ -27,13 +29,18 @@ import argparse
 import json
 import math
 import os
+import sys
 import tempfile
 import time
 
 import numpy as np
 import torch
 
-from . import configs, kernels
+HERE = os.path.dirname(os.path.abspath(__file__))
+if HERE not in sys.path:
+    sys.path.insert(0, HERE)
+
+from openonda_b200 import configs, kernels  # noqa: E402
 
 
 def _emit(d):
@@ -63,7 +70,7 @@ class _Timer:
 
 
 def _system(field, precision, **kw):
-    from .vpm.vpmModule import ParticleSystem
+    from openonda_b200.vpm.vpmModule import ParticleSystem
 
     # the reference backs up at time step 0 (0 % frequency == 0): keep that file out of cwd
     ps = ParticleSystem(monitor_variables=[], backup_frequency=10 ** 9, precision=precision,
@@ -180,7 +187,7 @@ def config3(args):
 
 
 def config4(args):
-    from . import autodiff
+    from openonda_b200 import autodiff
 
     f = configs.perturbed_ring()
     r = lambda z: torch.from_numpy(np.asarray(z, np.float32).astype(np.float64)).cuda()
@@ -337,7 +344,7 @@ def peaks(args):
 
 
 def stepkernels(args):
-    from . import _lib
+    from openonda_b200 import _lib
 
     lib = _lib.load()
     n = args.n or (1 << 22)
@@ -371,10 +378,120 @@ def stepkernels(args):
                "gb_s": round(bytes_per * n / (ms / 1e3) / 1e9, 1)})
 
 
+def _reference_module(name):
+    sys.path.insert(0, os.path.join(HERE, "baseline"))
+    from install_ref import load_reference_module
+
+    return load_reference_module(name)
+
+
+def reference(args):
+    """The reference's own code timed on this box, on the random cloud of the throughput
+    sweep: its Numba-CUDA kernels (ParticlesPhysicsCuda.py, unmodified, from baseline/_ref) on
+    the GPU -- kernel time by CUDA events and end to end through its module functions, which
+    copy inputs in and results out on every call -- and its Numba CPU module
+    (ParticlesPhysics.py) on all host cores.  Each result is compared with this library's FP64
+    drop-in on the same inputs."""
+    n = args.n or 131072
+    f = configs.random_cloud(n, seed=0)
+    x, a, s, nu = (np.ascontiguousarray(z) for z in (f.positions, f.strengths, f.radii,
+                                                     f.viscosities))
+    dev = torch.device("cuda")
+    tx, ta, ts, tn = (torch.from_numpy(z).to(dev) for z in (x, a, s, nu))
+    ours = {
+        "velocity": kernels.selfinduced_velocity(tx, ta, ts, precision="fp64"),
+        "stretching": kernels.strength_gradients(tx, ta, ts, precision="fp64"),
+        "pse": kernels.strength_gradients_pse(tx, ta, ts, tn, precision="fp64"),
+    }
+    ours = {k: v.cpu().numpy() for k, v in ours.items()}
+    try:
+        import numba
+        from numba import cuda
+
+        t0 = time.perf_counter()
+        mod = _reference_module("ParticlesPhysicsCuda")
+        jit_s = time.perf_counter() - t0
+        cc = cuda.get_current_device().compute_capability
+    except Exception as e:  # noqa: BLE001 -- report why, do not fail the run
+        _emit({"reference_gpu": "unavailable on this box",
+               "error": f"{type(e).__name__}: {str(e).splitlines()[0] if str(e) else ''}"})
+        mod = None
+    if mod is not None:
+        xd, ad, sd, nd = (cuda.to_device(z) for z in (x, a, s, nu))
+        od = cuda.device_array_like(x)
+        blocks = (n + mod.threads_per_block - 1) // mod.threads_per_block
+        cases = {
+            "velocity": (mod.get_selfinduced_velocity_kernel, (xd, ad, sd, od),
+                         lambda: mod.get_selfinduced_velocity(x, a, s)),
+            "stretching": (mod.get_strength_gradients_kernel, (xd, ad, sd, od),
+                           lambda: mod.get_strength_gradients(x, a, s)),
+            "pse": (mod.get_strength_gradients_PSE_kernel, (xd, ad, sd, nd, od),
+                    lambda: mod.get_strength_gradients_PSE(x, a, s, nu)),
+        }
+        for name, (kern, kargs, wrapper) in cases.items():
+            kern[blocks, mod.threads_per_block](*kargs)  # first launch loads the module
+            cuda.synchronize()
+            e0, e1 = cuda.event(), cuda.event()
+            e0.record()
+            kern[blocks, mod.threads_per_block](*kargs)
+            e1.record()
+            e1.synchronize()
+            ms = cuda.event_elapsed_time(e0, e1)
+            got_kernel = od.copy_to_host()
+            t0 = time.perf_counter()
+            got = wrapper()
+            e2e_s = time.perf_counter() - t0
+            _emit({"reference_gpu": name, "n": n, "numba": numba.__version__,
+                   "device_cc": list(cc), "module_import_and_jit_s": round(jit_s, 1),
+                   "kernel_ms": round(ms, 2),
+                   "kernel_gpairs_per_s": round(float(n) * n / (ms / 1e3) / 1e9, 3),
+                   "e2e_ms": round(e2e_s * 1e3, 2),
+                   "e2e_gpairs_per_s": round(float(n) * n / e2e_s / 1e9, 3),
+                   "rel_diff_ours_fp64_vs_reference": _rel(ours[name], got),
+                   "rel_diff_kernel_vs_wrapper": _rel(got_kernel, got)})
+    # the reference's CPU module, all host cores (Numba parallel), on target subsets
+    try:
+        import numba
+
+        cpu = _reference_module("ParticlesPhysics")
+    except Exception as e:  # noqa: BLE001
+        _emit({"reference_cpu": "unavailable on this box",
+               "error": f"{type(e).__name__}: {e}"})
+        return
+    threads = numba.get_num_threads()
+    m = 64
+    cpu.get_induced_velocity_at(x[:m], x[:m], a[:m], s[:m])  # JIT
+    t0 = time.perf_counter()
+    cpu.get_induced_velocity_at(x[:m], x, a, s)
+    rate = m * n / (time.perf_counter() - t0)
+    m = int(min(n, max(64, rate * (args.cpu_seconds or 5.0) / n)))
+    t0 = time.perf_counter()
+    got = cpu.get_induced_velocity_at(x[:m], x, a, s)
+    dt = time.perf_counter() - t0
+    _emit({"reference_cpu": "velocity (get_induced_velocity_at, target rows x all sources)",
+           "n_sources": n, "n_targets": m, "threads": threads, "s": round(dt, 2),
+           "gpairs_per_s": round(m * n / dt / 1e9, 4)})
+    ns = min(n, args.cpu_n or 16384)
+    xs, as_, ss, nus = x[:ns], a[:ns], s[:ns], nu[:ns]
+    for name, fn in (("stretching", lambda: cpu.get_strength_gradients(xs, as_, ss)),
+                     ("pse", lambda: cpu.get_strength_gradients_PSE(xs, as_, ss, nus))):
+        if name == "stretching":
+            cpu.get_strength_gradients(xs[:64], as_[:64], ss[:64])  # JIT
+        else:
+            cpu.get_strength_gradients_PSE(xs[:64], as_[:64], ss[:64], nus[:64])
+        t0 = time.perf_counter()
+        fn()
+        dt = time.perf_counter() - t0
+        _emit({"reference_cpu": name, "n": ns, "threads": threads, "s": round(dt, 2),
+               "gpairs_per_s": round(float(ns) * ns / dt / 1e9, 4)})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("workload", choices=["config1", "config2", "config3", "config4", "config5",
-                                         "stepkernels", "sweeps", "peaks"])
+                                         "stepkernels", "sweeps", "peaks", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=None)
+    ap.add_argument("--cpu-n", type=int, default=None)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--fd", type=int, default=None)
     ap.add_argument("--n", type=int, default=None)
