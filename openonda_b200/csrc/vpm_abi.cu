@@ -386,7 +386,7 @@ struct RotSweep {
   static constexpr int NV = Op::NV;
   static constexpr int kMaxPairs = 8;
   static constexpr int kTile = rot_tile<Op>();
-  static constexpr size_t kSmem = rot_smem_bytes(NV, kTile);
+  static constexpr size_t kSmem = rot_smem_bytes<Op>();
   static int64_t tiles(int64_t n) { return (n + kTile - 1) / kTile; }
   static size_t set_bytes(int64_t n) { return size_t(NV) * size_t(n) * sizeof(double); }
 
@@ -839,6 +839,8 @@ int run(const Call& c) {
       if (rc) return rc;
       double scale = 1.0 / (8.0 * kPi);
       if (c.ref_extra_4pi) scale /= 4.0 * kPi;
+      // the both-sides sweep sums the symmetric enstrophy term once per unordered pair
+      if (p.pairs) scale *= 2.0;
       finalize_dot_kernel<T, Op::NV, 12><<<1, kReduceThreads, 0, c.st>>>(part, p.splits, c.m,
                                                                           tgt, scale, c.out4);
       cudaError_t e = cudaGetLastError();

@@ -129,9 +129,12 @@ __host__ __device__ constexpr int rot_tile() {
 #define VPM_ROT_TGT_WINDOW 32
 #endif
 
-constexpr size_t rot_smem_bytes(int nv, int tile) {
-  return size_t(tile) * nv * sizeof(double) +                // target-side FP64 carries
-         size_t(2) * kRotWarps * 32 * nv * sizeof(float2);  // source-side sums, double-buffered
+// Dynamic shared memory of one CTA: the target-side FP64 carries [NV][T], then the
+// source-side sums of the first kSymFrom values, [kJBufs][kSymFrom][warps * 32].
+template <class Op>
+constexpr size_t rot_smem_bytes() {
+  return size_t(rot_tile<Op>()) * Op::NV * sizeof(double) +
+         size_t(Op::kJBufs) * Op::kSymFrom * kRotWarps * 32 * sizeof(float2);
 }
 
 // The source a lane holds on the standard 64-byte record: position, core, strength.
@@ -198,6 +201,8 @@ struct OpVelStretchBoth : RotStd<OpVelStretch<float2, REFINE, UC>, UC> {
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   static constexpr int kSrcWindow = VPM_ROT_SRC_WINDOW;
   static constexpr int kTgtWindow = VPM_ROT_TGT_WINDOW;
+  static constexpr int kSymFrom = NV;  // every sum has a source side
+  static constexpr int kJBufs = 2;     // double-buffered source-side sums
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -250,6 +255,8 @@ struct OpVelBoth : RotStd<OpVel<float2, REFINE, UC>, UC> {
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   static constexpr int kSrcWindow = VPM_ROT3_SRC_WINDOW;
   static constexpr int kTgtWindow = 32;
+  static constexpr int kSymFrom = NV;
+  static constexpr int kJBufs = 2;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -288,6 +295,8 @@ struct OpPseBoth : RotStd<OpPse<float2, REFINE, UC>, UC> {
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   static constexpr int kSrcWindow = VPM_ROT3_SRC_WINDOW;
   static constexpr int kTgtWindow = 32;
+  static constexpr int kSymFrom = NV;
+  static constexpr int kJBufs = 2;
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -327,6 +336,11 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
   static constexpr int kUnroll = VPM_ROT15_UNROLL;
   static constexpr int kSrcWindow = VPM_ROT_SRC_WINDOW;
   static constexpr int kTgtWindow = VPM_ROT_TGT_WINDOW;
+  // values 12-14 (enstrophy filter sum) are taken once per unordered pair, target side only
+  static constexpr int kSymFrom = 12;
+  // three resident CTAs fit the shared memory only with one buffer of source-side sums
+  static constexpr int kJBufs = VPM_ROT15_MINB >= 3 ? 1 : 2;
+  __device__ __forceinline__ static constexpr bool carried(int v) { return v < kSymFrom; }
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -393,14 +407,13 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
     jv[9] = fma(-kj, t.ax, jv[9]);
     jv[10] = fma(-kj, t.ay, jv[10]);
     jv[11] = fma(-kj, t.az, jv[11]);
-    // enstrophy filter sum (pair core)
+    // enstrophy filter sum (pair core): only the scalar sum_i a_i . E_i is wanted and the pair
+    // term is symmetric, so target i takes the pair once and the finalize doubles it; particle
+    // j takes nothing (the diagonal tiles, visited one-sided, are folded at half weight)
     const V ke = fma(splat<V>(2.2), s2, x) * y3;
     acc[12] = fma(ke, s.ax, acc[12]);
     acc[13] = fma(ke, s.ay, acc[13]);
     acc[14] = fma(ke, s.az, acc[14]);
-    jv[12] = fma(-ke, t.ax, jv[12]);
-    jv[13] = fma(-ke, t.ay, jv[13]);
-    jv[14] = fma(-ke, t.az, jv[14]);
   }
 };
 
@@ -437,6 +450,8 @@ struct OpRhsVjpBoth {
   static constexpr int kUnroll = PSE ? VPM_ROTGP_UNROLL : VPM_ROTG_UNROLL;
   static constexpr int kSrcWindow = VPM_ROTG_SRC_WINDOW;
   static constexpr int kTgtWindow = 32;
+  static constexpr int kSymFrom = NV;
+  static constexpr int kJBufs = 2;
 
   __device__ __forceinline__ static Lane load_lane(const Record* rec, int64_t j, int64_t n) {
     if (j < n) {
@@ -598,6 +613,7 @@ rot_sweep_kernel(const RotArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* car = reinterpret_cast<double*>(smem_raw);  // [NV][T]
   // [2][NV][WT]: each warp's packed source-side sums of the current batch, per source
+  constexpr int NJ = Op::kSymFrom;  // values with a source side: the first NJ
   float2* jbuf = reinterpret_cast<float2*>(smem_raw + size_t(T) * NV * sizeof(double));
   const Record* rec = static_cast<const Record*>(a.rec);
 
@@ -655,7 +671,7 @@ rot_sweep_kernel(const RotArgs a) {
     float2 jv[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) jv[v] = make_float2(0.f, 0.f);
-    float2* jb = jbuf + (b & 1) * (NV * WT);
+    float2* jb = jbuf + (b % Op::kJBufs) * (NJ * WT);
     const int src_lane = (lane + 1) & 31;
     for (int w = 0; w < 32 / SW; ++w) {
 #pragma unroll Op::kUnroll
@@ -707,17 +723,24 @@ rot_sweep_kernel(const RotArgs a) {
         for (int p = 0; p < P; ++p) {
 #pragma unroll
           for (int v = 0; v < NV; ++v) {
-            car[v * T + lt[2 * p]] += double(acc[p][v].x);
-            car[v * T + lt[2 * p + 1]] += double(acc[p][v].y);
+            if (DIAG && v >= NJ) {
+              // a symmetric sum taken once per unordered pair elsewhere: the diagonal tiles
+              // visit every ordered pair, so they count half (the finalize doubles the sum)
+              car[v * T + lt[2 * p]] += 0.5 * double(acc[p][v].x);
+              car[v * T + lt[2 * p + 1]] += 0.5 * double(acc[p][v].y);
+            } else {
+              car[v * T + lt[2 * p]] += double(acc[p][v].x);
+              car[v * T + lt[2 * p + 1]] += double(acc[p][v].y);
+            }
             acc[p][v] = make_float2(0.f, 0.f);
           }
         }
       }
     }
     if constexpr (!DIAG) {
-      __syncthreads();  // one barrier per batch; jbuf is double-buffered
+      __syncthreads();  // the batch's source-side sums are complete
       const int nsrc = (cnt - b * 32 < 32) ? cnt - b * 32 : 32;
-      for (int q = tid; q < 32 * NV; q += kRotThreads) {
+      for (int q = tid; q < 32 * NJ; q += kRotThreads) {
         const int v = q >> 5, jj = q & 31;  // consecutive threads: consecutive sources
         if (jj >= nsrc || !Op::carried(v)) continue;
         // both packed halves of every warp's sum, in FP64, in a fixed order
@@ -732,6 +755,8 @@ rot_sweep_kernel(const RotArgs a) {
         // adds in a fixed order (launch order) and the thread does not wait for the load
         atomicAdd(&a.acc[(int64_t(set_j) * NV + v) * a.n + (j0 + b * 32 + jj)], -sum);
       }
+      // one buffer: every thread has read it before the next batch writes it
+      if constexpr (Op::kJBufs == 1) __syncthreads();
     }
   }
   __syncthreads();
