@@ -235,6 +235,24 @@ size_t vpm_les_workspace_bytes(int64_t n);
 int vpm_les_update(const double* vorticity, const double* radii, const double* enstrophy,
                    int64_t n, int advance_constant, double* les_state, double* viscosities_t,
                    double* nut_max, void* workspace, size_t workspace_bytes, void* stream);
+/* Least-squares dynamic LES coefficient, FP64 (no counterpart in the reference, which only
+ * rescales Cnu by its enstrophy ratio, vpmModule.py:887-909).  Germano identity for the
+ * sub-filter kinetic energy k(D) = C^2 D^2 |w_D|^2 between the particle filter (core sigma) and
+ * a test filter of core 2 sigma:
+ *   L_i = (hat(|u|^2)_i - |hat u_i|^2) / 2,   M_i = (2 sigma_i)^2 |hat w_i|^2 - hat(sigma^2|w|^2)_i,
+ *   Cnu = clip(sqrt(sum L M / sum M M), 1e-9, 0.0761)  (unchanged when either sum is <= 0).
+ * vpm_les_lsq_weights writes the per-particle fields the test filter acts on, times the particle
+ * volume |alpha|/|w|: weights (n,3) = (|u|^2 v, sigma^2 |w|^2 v, 0).  The caller forms, with the
+ * pair-sum entry points and radii 2 sigma: hat u = vpm_selfinduced_velocity, hat w =
+ * vpm_vorticity_field_at(x, x, alpha, 2 sigma), hat f = vpm_vorticity_field_at(x, x, weights,
+ * 2 sigma).  vpm_les_lsq_update reduces both sums in one block in a fixed order, writes them to
+ * `sums` (2 device doubles, may be NULL) and updates les_state[0] (= Cnu) on the device. */
+int vpm_les_lsq_weights(const double* velocities, const double* vorticity,
+                        const double* strengths, const double* radii, int64_t n,
+                        double* weights, void* stream);
+int vpm_les_lsq_update(const double* test_velocities, const double* test_vorticity,
+                       const double* test_filtered, const double* radii, int64_t n,
+                       double* les_state, double* sums, void* stream);
 /* Strength relaxation towards the vorticity direction, in place (vpmModule.py:867-883). */
 int vpm_relax_strengths(double* strengths, const double* vorticity, int64_t n, double alpha,
                         void* stream);

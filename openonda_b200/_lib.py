@@ -78,6 +78,8 @@ SIGNATURES = {
     "vpm_core_spreading": ([_P, _P, _P, _I64, ctypes.c_double, ctypes.c_double, _P], _I),
     "vpm_les_workspace_bytes": ([_I64], _SZ),
     "vpm_les_update": ([_P, _P, _P, _I64, _I, _P, _P, _P, _P, _SZ, _P], _I),
+    "vpm_les_lsq_weights": ([_P, _P, _P, _P, _I64, _P, _P], _I),
+    "vpm_les_lsq_update": ([_P, _P, _P, _P, _I64, _P, _P, _P], _I),
     "vpm_relax_strengths": ([_P, _P, _I64, ctypes.c_double, _P], _I),
     "vpm_particle_diagnostics": ([_P, _P, _I64, _P, _P], _I),
     "vpm_ic_workspace_bytes": ([_I64], _SZ),

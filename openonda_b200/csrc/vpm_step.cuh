@@ -241,6 +241,74 @@ diagnostics_kernel(const double* __restrict__ x, const double* __restrict__ a, i
   }
 }
 
+// ---- least-squares dynamic coefficient (no counterpart in the reference) ------------------
+// Germano identity for the sub-filter kinetic energy between the particle filter (core sigma)
+// and a test filter of twice the core, with the model k(D) = C^2 D^2 |w_D|^2 (w_D: vorticity
+// filtered at width D):
+//   L_i = 1/2 (hat(|u|^2)_i - |hat u_i|^2)        resolved energy between the two filters
+//   M_i = (2 sigma_i)^2 |hat w_i|^2 - hat(sigma^2 |w|^2)_i
+//   C^2 = sum_i L_i M_i / sum_i M_i^2             (least squares over all particles, FP64)
+// hat f_i = sum_j zeta_{2 sigma_j}(x_i - x_j) f_j v_j is the test filter of a particle field,
+// with the particle volume v_j = |alpha_j| / |w_j| (0 where w_j = 0).  Cnu = sqrt(C^2) clipped to
+// the reference's range [1e-9, 0.0761]; where C^2 <= 0 or sum M^2 = 0 Cnu stays unchanged.
+
+// w_j = (|u_j|^2 v_j, sigma_j^2 |w_j|^2 v_j, 0): the fields the test filter acts on.
+__global__ void les_lsq_weights_kernel(const double* __restrict__ u, const double* __restrict__ w,
+                                       const double* __restrict__ a,
+                                       const double* __restrict__ sigma, int64_t n,
+                                       double* __restrict__ out) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double ux = u[3 * i], uy = u[3 * i + 1], uz = u[3 * i + 2];
+  const double wx = w[3 * i], wy = w[3 * i + 1], wz = w[3 * i + 2];
+  const double ax = a[3 * i], ay = a[3 * i + 1], az = a[3 * i + 2];
+  const double w2 = wx * wx + wy * wy + wz * wz;
+  const double vol = w2 > 0.0 ? sqrt(ax * ax + ay * ay + az * az) / sqrt(w2) : 0.0;
+  const double s = sigma[i];
+  out[3 * i] = (ux * ux + uy * uy + uz * uz) * vol;
+  out[3 * i + 1] = s * s * w2 * vol;
+  out[3 * i + 2] = 0.0;
+}
+
+// Single block, fixed order: sum L M and sum M M, then the coefficient update.
+__global__ void __launch_bounds__(1024)
+les_lsq_kernel(const double* __restrict__ uh, const double* __restrict__ wh,
+               const double* __restrict__ fh, const double* __restrict__ sigma, int64_t n,
+               double* __restrict__ st, double* __restrict__ sums) {
+  __shared__ double red[2][1024];
+  double lm = 0.0, mm = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += 1024) {
+    const double hx = uh[3 * i], hy = uh[3 * i + 1], hz = uh[3 * i + 2];
+    const double gx = wh[3 * i], gy = wh[3 * i + 1], gz = wh[3 * i + 2];
+    const double L = 0.5 * (fh[3 * i] - (hx * hx + hy * hy + hz * hz));
+    const double d = 2.0 * sigma[i];
+    const double M = d * d * (gx * gx + gy * gy + gz * gz) - fh[3 * i + 1];
+    lm += L * M;
+    mm += M * M;
+  }
+  red[0][threadIdx.x] = lm;
+  red[1][threadIdx.x] = mm;
+  __syncthreads();
+  for (int k = 512; k > 0; k >>= 1) {
+    if (threadIdx.x < k) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + k];
+      red[1][threadIdx.x] += red[1][threadIdx.x + k];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double slm = red[0][0], smm = red[1][0];
+    if (sums) {
+      sums[0] = slm;
+      sums[1] = smm;
+    }
+    if (smm > 0.0 && slm > 0.0) {
+      const double c = sqrt(slm / smm);
+      st[0] = fmax(kModuleEps, fmin(c, 0.0761));
+    }
+  }
+}
+
 int launch_status(const char* what) {
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? VPM_OK : cuda_fail(e, what);
@@ -335,6 +403,30 @@ int vpm_les_update(const double* vorticity, const double* radii, const double* e
   les_commit_kernel<<<nb < 1184 ? nb : 1184, kEwThreads, 0, st>>>(nut_new, bmax, int(nb), n,
                                                                    viscosities_t, nut_max);
   return launch_status("les commit launch");
+}
+
+int vpm_les_lsq_weights(const double* velocities, const double* vorticity,
+                        const double* strengths, const double* radii, int64_t n,
+                        double* weights, void* stream) {
+  using namespace vpm;
+  if (n < 0 || (n > 0 && (!velocities || !vorticity || !strengths || !radii || !weights)))
+    return fail(VPM_ERR_ARG, "bad les lsq weights args");
+  if (n == 0) return VPM_OK;
+  les_lsq_weights_kernel<<<ew_blocks(n), kEwThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      velocities, vorticity, strengths, radii, n, weights);
+  return launch_status("les lsq weights launch");
+}
+
+int vpm_les_lsq_update(const double* test_velocities, const double* test_vorticity,
+                       const double* test_filtered, const double* radii, int64_t n,
+                       double* les_state, double* sums, void* stream) {
+  using namespace vpm;
+  if (n < 0 || !les_state ||
+      (n > 0 && (!test_velocities || !test_vorticity || !test_filtered || !radii)))
+    return fail(VPM_ERR_ARG, "bad les lsq args");
+  les_lsq_kernel<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(
+      test_velocities, test_vorticity, test_filtered, radii, n, les_state, sums);
+  return launch_status("les lsq launch");
 }
 
 int vpm_relax_strengths(double* strengths, const double* vorticity, int64_t n, double alpha,

@@ -91,7 +91,8 @@ class ParticleSystem:
                  viscous_scheme: str = "CoreSpreading", monitor_variables=None,
                  flow_time: float = 0.0, time_step: int = 0, backup_frequency: int = 1,
                  backup_filename: str = "particle_data", relax_strength_solution: bool = False,
-                 precision: str = "fp64", device=None, verbose: bool = False):
+                 precision: str = "fp64", device=None, verbose: bool = False,
+                 les_coefficient: str = "reference"):
         if monitor_variables is None:
             monitor_variables = ["Circulation", "Linear Impulse", "Angular Impulse",
                                  "Kinetic Energy", "Enstrophy", "Helicity"]
@@ -101,6 +102,9 @@ class ParticleSystem:
         self._validate_viscous_scheme(viscous_scheme)
         self._validate_processing_unit(processing_unit)
         _lib.precision_code(precision)
+        if les_coefficient not in ("reference", "least_squares"):
+            raise ValueError("Invalid LES coefficient scheme. Choose 'reference' or "
+                             "'least_squares'.")
 
         self.time_step_size = time_step_size
         self.flow_time = flow_time
@@ -114,6 +118,10 @@ class ParticleSystem:
         self.processing_unit = processing_unit
         self.relax_strength_solution = relax_strength_solution
         self.precision = precision
+        # "reference": Cnu rescaled by its enstrophy ratio (vpmModule.py:887-909);
+        # "least_squares": Germano-identity least squares in FP64 (no counterpart in the
+        # reference; see _les_least_squares)
+        self.les_coefficient = les_coefficient
         self.verbose = verbose
         self.device = torch.device(device) if device is not None else None
 
@@ -654,7 +662,7 @@ class ParticleSystem:
         ts += list(self._hist or [])
         return (self._n, float(self.time_step_size), self.time_integration_method.strip(),
                 self.flow_model, self.viscous_scheme, self.precision, self._uc,
-                bool(self.relax_strength_solution),
+                bool(self.relax_strength_solution), self.les_coefficient,
                 tuple(0 if t is None else t.data_ptr() for t in ts))
 
     def _prime_plans(self):
@@ -760,8 +768,13 @@ class ParticleSystem:
                 w = self._vorticity()
                 ens = kernels.total_enstrophy(self._x, self._a, self._s, ref_extra_4pi=True,
                                               precision=self.precision, uniform_core=self._uc)
+            u = self._u if self._rate_token == self._token and self._u is not None else None
             self._les_w = self._les_ens = None
-            self._les_update(w, ens)
+            if self.les_coefficient == "least_squares":
+                self._les_least_squares(w, u)
+                self._les_update(w, None, advance_constant=False)
+            else:
+                self._les_update(w, ens)
         rate_s = None
         if self.flow_model in ("LES", "DNS"):
             rate_s = self._stretching_rate()
@@ -804,6 +817,30 @@ class ParticleSystem:
             int(advance_constant), st.data_ptr(), self._nut.data_ptr(), nut_max.data_ptr(),
             ws.data_ptr(), ws.numel(), _stream(dev)))
         self._nut_max = nut_max
+
+    def _les_least_squares(self, vorticity, velocities=None):
+        """Cnu from the Germano identity for the sub-filter kinetic energy between the particle
+        filter (core sigma) and a test filter of core 2 sigma, by least squares over all
+        particles in FP64 (vpm_les_lsq_update).  Three extra sweeps: the test-filtered
+        velocity, vorticity and the test filter of (|u|^2, sigma^2 |w|^2) times the particle
+        volume.  Returns the device sums (sum L M, sum M M)."""
+        dev = self._dev()
+        lib = _lib.load()
+        st = _stream(dev)
+        u = velocities if velocities is not None else self._vel(self._x)
+        s2 = 2.0 * self._s
+        uh = kernels.selfinduced_velocity(self._x, self._a, s2, precision=self.precision,
+                                          uniform_core=self._uc)
+        wh = kernels.vorticity_field_at(self._x, self._x, self._a, s2, precision=self.precision)
+        wts = torch.empty_like(self._a)
+        _check(lib.vpm_les_lsq_weights(u.data_ptr(), vorticity.data_ptr(), self._a.data_ptr(),
+                                       self._s.data_ptr(), self._n, wts.data_ptr(), st))
+        fh = kernels.vorticity_field_at(self._x, self._x, wts, s2, precision=self.precision)
+        sums = torch.empty(2, dtype=_F64, device=dev)
+        _check(lib.vpm_les_lsq_update(uh.data_ptr(), wh.data_ptr(), fh.data_ptr(),
+                                      self._s.data_ptr(), self._n, self._les_state().data_ptr(),
+                                      sums.data_ptr(), st))
+        return sums
 
     def _update_LES_filter_constant(self, enstrophy: float):
         """Dynamic constant update from an enstrophy value (vpmModule.py:887-909)."""

@@ -81,8 +81,8 @@ def test_both_sides_vs_fp64(n, ring, uniform_core):
                                                         uniform_core=uniform_core)
         ref = kernels.velocity_and_strength_gradients(x, a, s, precision="fp64")
         kernels.set_symmetric_min_n(0)
-        plan = kernels.plan_info("velocity_and_strength_gradients", "fp32c", n, n)
-        assert plan["splits"] % 4 == 0 and plan["threads"] == 128  # the both-sides plan
+        # the both-sides plan: zeroing, diagonal-pair launches, finalize
+        assert kernels.sweep_launches("velocity_and_strength_gradients", "fp32c", n, n) > 2
         both = kernels.velocity_and_strength_gradients(x, a, s, precision="fp32c",
                                                        uniform_core=uniform_core)
     finally:
@@ -163,8 +163,7 @@ def test_velocity_and_pse_both_sides_vs_fp64(op, n, ring, uniform_core):
         one32 = fn(*args, precision="fp32c", uniform_core=uniform_core)
         ref = fn(*args, precision="fp64")
         kernels.set_symmetric_min_n(0)
-        plan = kernels.plan_info(op, "fp32c", n, n)
-        assert plan["splits"] % 4 == 0 and plan["threads"] == 128  # the both-sides plan
+        assert kernels.sweep_launches(op, "fp32c", n, n) > 2  # the both-sides plan
         both = fn(*args, precision="fp32c", uniform_core=uniform_core)
         again = fn(*args, precision="fp32c", uniform_core=uniform_core)
     finally:
@@ -182,11 +181,11 @@ def test_helicity_and_shards_stay_one_sided(both_sides_always):
     from openonda_b200 import kernels
 
     n = 4096
-    assert kernels.plan_info("selfinduced_velocity", "fp32c", n, n)["splits"] % 4 == 0
+    assert kernels.sweep_launches("selfinduced_velocity", "fp32c", n, n) > 2
     assert kernels.sweep_launches("total_helicity", "fp32c", n, n) == 2
     assert kernels.sweep_launches("selfinduced_velocity", "fp32c", 1000, n) == 2
     assert kernels.sweep_launches("strength_gradients_pse", "fp64", n, n) == 2
-    assert kernels.sweep_launches("strength_gradients_pse", "fp32c", n, n) > 3
+    assert kernels.sweep_launches("strength_gradients_pse", "fp32c", n, n) > 2
 
 
 @pytest.mark.parametrize("n,ring", [(ONE_PAST_TILE, False), (1000, False), (3001, False),
@@ -211,8 +210,7 @@ def test_les_step_sums_both_sides_vs_fp64(n, ring, uniform_core):
         one32 = kernels.les_step_sums(x, a, s, precision="fp32c", uniform_core=uniform_core)
         ref = kernels.les_step_sums(x, a, s, precision="fp64")
         kernels.set_symmetric_min_n(0)
-        plan = kernels.plan_info("les_step_sums", "fp32c", n, n)
-        assert plan["splits"] % 4 == 0 and plan["threads"] == 128  # the both-sides plan
+        assert kernels.sweep_launches("les_step_sums", "fp32c", n, n) > 2  # both-sides plan
         both = kernels.les_step_sums(x, a, s, precision="fp32c", uniform_core=uniform_core)
         again = kernels.les_step_sums(x, a, s, precision="fp32c", uniform_core=uniform_core)
     finally:
@@ -252,7 +250,7 @@ def test_rhs_vjp_both_sides_vs_fp64(n, ring, pse):
         one32 = autodiff.rhs_vjp(x, a, s, nu, gu, gs, "fp32c")
         ref = autodiff.rhs_vjp(x, a, s, nu, gu, gs, "fp64")
         kernels.set_symmetric_min_n(0)
-        assert kernels.sweep_launches(op, "fp32c", n, n) > 3  # the both-sides plan
+        assert kernels.sweep_launches(op, "fp32c", n, n) > 2  # the both-sides plan
         both = autodiff.rhs_vjp(x, a, s, nu, gu, gs, "fp32c")
         again = autodiff.rhs_vjp(x, a, s, nu, gu, gs, "fp32c")
     finally:
@@ -276,7 +274,7 @@ def test_refined_rsqrt_both_sides(both_sides_always):
     x, a, s = _dev32(f)
     nu = torch.from_numpy(np.ascontiguousarray(f.viscosities)).cuda()
     p = "fp32c_refined"
-    assert kernels.sweep_launches("velocity_and_strength_gradients", p, n, n) > 3
+    assert kernels.sweep_launches("velocity_and_strength_gradients", p, n, n) > 2
     pairs = [
         (kernels.velocity_and_strength_gradients(x, a, s, precision=p),
          kernels.velocity_and_strength_gradients(x, a, s, precision="fp64"), (1e-6, 2e-6)),

@@ -21,6 +21,9 @@ def test_constructor_validation_messages():
         v.ParticleSystem(processing_unit="CPU")
     with pytest.raises(ValueError, match="unknown precision"):
         v.ParticleSystem(precision="fp16")
+    with pytest.raises(ValueError, match="Invalid LES coefficient scheme"):
+        v.ParticleSystem(flow_model="LES", viscous_scheme="PSE", les_coefficient="germano")
+    assert v.ParticleSystem().les_coefficient == "reference"
 
 
 def test_defaults_follow_the_reference():

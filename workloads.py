@@ -163,8 +163,37 @@ def config2(args):
            "gpairs_per_s": round(pairs / (t_total / steps / 1e3) / 1e9, 1), "checkpoints": rows})
 
 
+def _pipe_peaks():
+    """In-run microbenchmark peaks (lane-ops/s): scalar FFMA, packed FFMA2, MUFU rsqrt, FP64
+    DFMA; 8 blocks of 256 threads per SM, best of 5."""
+    dev = torch.device("cuda")
+    props = torch.cuda.get_device_properties(dev)
+    out = {}
+    for kind, name, lanes, dt in ((0, "ffma", 16, torch.float32), (3, "ffma2", 32, torch.float32),
+                                  (2, "mufu", 16, torch.float32), (1, "dfma", 16, torch.float64)):
+        blocks, threads, iters = props.multi_processor_count * 8, 256, 1 << 13
+        sink = torch.empty(blocks * threads, dtype=dt, device=dev)
+        kernels.launch_fma_peak(kind, blocks, threads, 64, sink)
+        best = float("inf")
+        for _ in range(5):
+            with _Timer() as t:
+                kernels.launch_fma_peak(kind, blocks, threads, iters, sink)
+            best = min(best, t.ms / 1e3)
+        out[name] = blocks * threads * iters * lanes / best
+    return out
+
+
+# FP32 lane-ops and MUFU rsqrt per ordered pair of the fused velocity + stretching sum
+# (general cores): one-sided OpVelStretch 38 / 1, both-sides OpVelStretchBoth 26.5 / 0.5;
+# FP64 one-sided: 38 FP64 ops (DFMA pipe) and one rsqrt() per pair.
+_FUSED_OPS = {"one-sided": (38.0, 1.0), "both-sides": (26.5, 0.5)}
+
+
 def config3(args):
     sizes = args.sizes or [1 << k for k in range(14, 22)]
+    peaks = _pipe_peaks()
+    _emit({"config": "config3", "peaks_lane_ops_per_s": {k: round(v / 1e12, 3) for k, v in
+                                                          peaks.items()}})
     for n in sizes:
         f = configs.random_cloud(n, seed=0)
         r = lambda z: torch.from_numpy(np.asarray(z, np.float32).astype(np.float64)).cuda()
@@ -179,9 +208,17 @@ def config3(args):
                     out[prec] = kernels.velocity_and_strength_gradients(x, a, s,
                                                                         precision=prec)
             res[prec] = n * n / (t.ms / reps / 1e3) / 1e9
+        path = ("both-sides" if kernels.sweep_launches("velocity_and_strength_gradients",
+                                                        "fp32c", n, n) > 2 else "one-sided")
+        ops, rsq = _FUSED_OPS[path]
+        r32 = res["fp32c"] * 1e9
         _emit({"config": "config3", "n": n, "fp32c_gpairs_s": round(res["fp32c"], 1),
                "fp64_gpairs_s": round(res["fp64"], 1),
-               "speedup": round(res["fp32c"] / res["fp64"], 2),
+               "speedup": round(res["fp32c"] / res["fp64"], 2), "fp32c_path": path,
+               "fp32_pipe_frac": round(r32 * ops / peaks["ffma"], 3),
+               "fp32_pipe_frac_of_packed": round(r32 * ops / peaks["ffma2"], 3),
+               "sfu_frac": round(r32 * rsq / peaks["mufu"], 3),
+               "fp64_pipe_frac_excl_rsqrt": round(res["fp64"] * 1e9 * 38.0 / peaks["dfma"], 3),
                "rel_err_velocity": _rel(out["fp32c"][0], out["fp64"][0]),
                "rel_err_stretching": _rel(out["fp32c"][1], out["fp64"][1])})
 
@@ -248,7 +285,8 @@ def config5(args):
     f = configs.les_ring()
     steps = args.steps or 100
     ps = _system(f, "fp32c", flow_model="LES", viscous_scheme="PSE",
-                 time_integration_method="RK4", time_step_size=0.002)
+                 time_integration_method="RK4", time_step_size=0.002,
+                 les_coefficient=args.les_coefficient)
     assert ps._uc  # one core for the whole ring: the uniform-core sweeps
     t_total = 0.0
     for k in range(steps):
@@ -262,6 +300,13 @@ def config5(args):
     les32 = kernels.les_step_sums(x32, a32, s32, precision="fp32c", uniform_core=ps._uc)
     ew = _rel(les32[2], les64[2])
     ee = abs(float(les32[3]) - float(les64[3])) / abs(float(les64[3]))
+    # both coefficient schemes on the final state: the one the run used, and the other
+    cnu_run = ps.Cnu
+    with _Timer() as tl:
+        sums = ps._les_least_squares(ps._vorticity())
+    cnu_lsq = ps.Cnu
+    ps.Cnu = cnu_run
+    lm, mm = (float(v) for v in sums.cpu())
     n = f.n
     # 7 N^2 pair sums per step as the reference counts them (velocity + stretching counted
     # once), run here as 5 sweeps: LES step sums (velocity, stretching, vorticity,
@@ -274,7 +319,12 @@ def config5(args):
            "gpairs_per_s": round(sums * n * n / (t_total / steps / 1e3) / 1e9, 1),
            "rel_err_velocity_last_step": eu, "rel_err_stretching_last_step": eg,
            "rel_err_vorticity_last_step": ew, "rel_err_enstrophy_last_step": ee,
-           "cnu": ps.Cnu})
+           "les_coefficient": args.les_coefficient, "cnu": cnu_run,
+           "cnu_least_squares_final_state": cnu_lsq,
+           "least_squares_sums": {"LM": lm, "MM": mm,
+                                  "C_unclipped": math.sqrt(lm / mm) if lm > 0 and mm > 0
+                                  else None},
+           "least_squares_ms": round(tl.ms, 1)})
 
 
 def sweeps(args):
@@ -491,6 +541,8 @@ def main():
     ap.add_argument("workload", choices=["config1", "config2", "config3", "config4", "config5",
                                          "stepkernels", "sweeps", "peaks", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=None)
+    ap.add_argument("--les-coefficient", default="reference",
+                    choices=["reference", "least_squares"])
     ap.add_argument("--cpu-n", type=int, default=None)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--fd", type=int, default=None)
