@@ -470,7 +470,8 @@ struct RotSweep {
     int rc = prepare(&occ);
     if (!rc) rc = zero_out(acc, int64_t(p.splits) * NV * n, st);
     if (rc) return rc;
-    rot_sweep_kernel<Op, true><<<nt, kRotThreads, kSmem, st>>>(RotArgs{rec, n, nt, 0, acc});
+    rot_sweep_kernel<Op, true><<<nt * kRotDiagSplit, kRotThreads, kSmem, st>>>(
+        RotArgs{rec, n, nt, 0, acc});
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
     const int npairs = nt / 2;

@@ -28,8 +28,9 @@
 // accumulator element has one writer per launch and the launches run in stream order, so the
 // atomic additions happen in a fixed order and the result is deterministic.  A launch runs m
 // consecutive diagonal pairs (m chosen so that its m * nt CTAs fill whole waves); launch 0
-// runs the diagonal tiles (I, I) one-sided into set 0.  The finalize pass sums the 4m sets in
-// order.
+// runs the diagonal tiles (I, I) one-sided, each in kRotDiagSplit CTAs that take a part of the
+// tile's sources each and add into sets 0 .. kRotDiagSplit - 1.  The finalize pass sums the 4m
+// sets in order.
 //
 // Accumulation: target side in FP32 per batch of 32 sources, folded into FP64 carries held in
 // shared memory; source side in FP32 over windows of kSrcWindow steps (each half of the
@@ -94,6 +95,9 @@ namespace vpm {
 #endif
 
 constexpr int kRotWarps = VPM_ROT_WARPS;
+// The diagonal tiles (one launch of their own) split their sources into this many parts, one
+// CTA each, so that the launch fills more of the GPU; part h adds into accumulator set h.
+constexpr int kRotDiagSplit = 4;
 constexpr int kRotThreads = 32 * kRotWarps;
 constexpr float kRotFar = 1e15f;  // position of the padding sources: every kernel underflows
 
@@ -619,10 +623,12 @@ rot_sweep_kernel(const RotArgs a) {
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int I, J, set_i, set_j;
+  int h = 0;  // DIAG: which part of the tile's sources this CTA takes
   if (DIAG) {
-    I = J = blockIdx.x;
-    set_i = 0;
-    set_j = 0;
+    I = J = blockIdx.x / kRotDiagSplit;
+    h = blockIdx.x - I * kRotDiagSplit;
+    set_i = h;  // each part into its own set: one writer per element
+    set_j = h;
   } else {
     const int q = blockIdx.x / a.nt, r = blockIdx.x - q * a.nt;
     const int k = a.k0 + q, n1 = a.nt - k;
@@ -640,8 +646,11 @@ rot_sweep_kernel(const RotArgs a) {
       return;  // k == nt - k: the diagonal has only nt - k tile pairs
     }
   }
-  const int64_t i0 = int64_t(I) * T, j0 = int64_t(J) * T;
-  const int cnt = int((a.n - j0 < T) ? (a.n - j0) : T);
+  // sources: the whole tile J, or (DIAG) part h of the diagonal tile
+  constexpr int TS = DIAG ? T / kRotDiagSplit : T;
+  static_assert(TS % 32 == 0, "source ranges are whole batches");
+  const int64_t i0 = int64_t(I) * T, j0 = int64_t(J) * T + int64_t(h) * TS;
+  const int cnt = int((a.n - j0 < TS) ? (a.n - j0 > 0 ? a.n - j0 : 0) : TS);
 
   for (int q = tid; q < T * NV; q += kRotThreads) car[q] = 0.0;
 
