@@ -83,7 +83,7 @@ constexpr size_t kMaxPartialBytes = size_t(4) << 30;
 
 struct Plan {
   int64_t tblocks = 0;
-  int splits = 1;  // source splits; the both-sides sweep: its accumulator sets (4 per pair)
+  int splits = 1;  // source splits; the both-sides sweep: its accumulator sets (2 per pair)
   int64_t chunk = 0;
   size_t smem = 0;
   int threads = 0;
@@ -384,19 +384,22 @@ int zero_out(double* p, int64_t count, cudaStream_t st) {
 template <class Op>
 struct RotSweep {
   static constexpr int NV = Op::NV;
-  static constexpr int kMaxPairs = 8;
+  static constexpr int kMaxPairs = 32;
   static constexpr int kTile = rot_tile<Op>();
   static constexpr size_t kSmem = rot_smem_bytes<Op>();
   static int64_t tiles(int64_t n) { return (n + kTile - 1) / kTile; }
   static size_t set_bytes(int64_t n) { return size_t(NV) * size_t(n) * sizeof(double); }
 
   // Whether the planner takes this sweep for a self sum of n particles: the size threshold
-  // (vpm_set_symmetric_min_n), two tiles at least, and the 4 accumulator sets of one diagonal
-  // pair within the caller's partial-sum budget.
+  // (vpm_set_symmetric_min_n), two tiles at least, and the smallest set count (that of the
+  // diagonal tiles' launch) within the caller's partial-sum budget.
   static bool usable(int64_t m, int64_t n, size_t max_partial_bytes) {
     return m == n && n >= g_sym_min_n.load() && tiles(n) >= 2 &&
-           4 * set_bytes(n) <= max_partial_bytes;
+           sets(1) * set_bytes(n) <= max_partial_bytes;
   }
+  // accumulator sets of a plan with m diagonal pairs per launch: 2 per pair, and at least the
+  // kRotDiagSplit the diagonal tiles' launch writes
+  static int64_t sets(int m) { return 2 * m > kRotDiagSplit ? 2 * m : kRotDiagSplit; }
 
   // Shared-memory attributes and resident CTAs per SM, once per device (cached like the
   // one-sided sweeps' plans).
@@ -441,7 +444,7 @@ struct RotSweep {
     int best_m = 1;
     double best = -1.0;
     for (int m = 1; m <= kMaxPairs && m <= npairs; ++m) {
-      if (m > 1 && 4 * m * set_bytes(n) > max_partial_bytes) break;
+      if (m > 1 && sets(m) * set_bytes(n) > max_partial_bytes) break;
       const double waves = double(m) * nt / slots;
       const double eff = waves / std::ceil(waves);
       if (eff > best + 1e-9) {
@@ -453,7 +456,7 @@ struct RotSweep {
     if (eff_out) *eff_out = best;
     p->pairs = best_m;
     p->tblocks = nt;
-    p->splits = 4 * best_m;
+    p->splits = int(sets(best_m));
     p->chunk = n;
     p->smem = kSmem;
     p->threads = kRotThreads;
@@ -462,7 +465,7 @@ struct RotSweep {
     return VPM_OK;
   }
 
-  // acc: [4 * pairs][NV][n] FP64, zeroed here.
+  // acc: [sets(pairs)][NV][n] FP64, zeroed here.
   static int launch(const Plan& p, const void* rec, int64_t n, double* acc,
                     cudaStream_t st) {
     const int nt = int(tiles(n));

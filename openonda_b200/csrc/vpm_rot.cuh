@@ -23,14 +23,15 @@
 // atomic.
 //
 // Tile-pair schedule: particles form nt tiles of T = 64 kP WARPS.  A CTA owns one tile pair
-// (I, J), I < J.  Diagonal pair q of a launch is J - I = k (accumulator sets 4q / 4q+1 for
-// the target / source side) together with J - I = nt - k (sets 4q+2 / 4q+3): every
-// accumulator element has one writer per launch and the launches run in stream order, so the
-// atomic additions happen in a fixed order and the result is deterministic.  A launch runs m
+// (I, J), I < J.  Diagonal pair q of a launch is J - I = k (accumulator sets 2q / 2q+1 for
+// the target / source side) together with J - I = nt - k (sets 2q+1 / 2q, on row ranges
+// disjoint from the first diagonal's): every accumulator element has one writer per launch
+// and the launches run in stream order, so the atomic additions happen in a fixed order and
+// the result is deterministic.  A launch runs m
 // consecutive diagonal pairs (m chosen so that its m * nt CTAs fill whole waves); launch 0
 // runs the diagonal tiles (I, I) one-sided, each in kRotDiagSplit CTAs that take a part of the
-// tile's sources each and add into sets 0 .. kRotDiagSplit - 1.  The finalize pass sums the 4m
-// sets in order.
+// tile's sources each and add into sets 0 .. kRotDiagSplit - 1.  The finalize pass sums the
+// max(2m, kRotDiagSplit) sets in order.
 //
 // Accumulation: target side in FP32 per batch of 32 sources, folded into FP64 carries held in
 // shared memory; source side in FP32 over windows of kSrcWindow steps (each half of the
@@ -632,16 +633,20 @@ rot_sweep_kernel(const RotArgs a) {
   } else {
     const int q = blockIdx.x / a.nt, r = blockIdx.x - q * a.nt;
     const int k = a.k0 + q, n1 = a.nt - k;
+    // Two sets per diagonal pair: the first diagonal's target rows [0, nt - k) and the
+    // second's source rows [nt - k, nt) share set 2q; the first's source rows [k, nt) and the
+    // second's target rows [0, k) share set 2q + 1.  The row ranges in a set are disjoint and
+    // each tile appears once per role, so every element still has one writer per launch.
     if (r < n1) {
       I = r;
       J = r + k;
-      set_i = 4 * q;
-      set_j = 4 * q + 1;
+      set_i = 2 * q;
+      set_j = 2 * q + 1;
     } else if (n1 > k) {
       I = r - n1;
       J = I + n1;
-      set_i = 4 * q + 2;
-      set_j = 4 * q + 3;
+      set_i = 2 * q + 1;
+      set_j = 2 * q;
     } else {
       return;  // k == nt - k: the diagonal has only nt - k tile pairs
     }
