@@ -161,7 +161,7 @@ int vpm_velocity_and_strength_gradients(const double* positions, const double* s
  * vpm_sweep_records over all records) with n >= this value evaluate each unordered pair once
  * for both particles (deterministic tile-pair schedule, about n / (2 T m) launches for tiles
  * of T = 512 or 768 particles and m diagonal pairs per launch).  Sets the threshold and
- * returns the previous one (default 65536).  No counterpart in the reference. */
+ * returns the previous one (default 24576).  No counterpart in the reference. */
 int64_t vpm_set_symmetric_min_n(int64_t n);
 /* Kernel launches of one sweep of `op` (sweep and finalize, not the packing of the inputs)
  * for m targets and n sources under the current plan; -1 on error. */

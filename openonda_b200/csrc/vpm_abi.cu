@@ -93,9 +93,11 @@ struct Plan {
   int variant = 0;  // both-sides fused sum: 0 = built for VPM_ROT_MINB CTAs/SM, 1 = _ALT
 };
 
-// FP32 self sums of velocity + stretching with at least this many particles evaluate each
-// unordered pair once for both particles (vpm_set_symmetric_min_n changes it).
-std::atomic<int64_t> g_sym_min_n{int64_t(1) << 16};
+// FP32 self sums with at least this many particles evaluate each unordered pair once for both
+// particles (vpm_set_symmetric_min_n changes it).  Measured crossover of the fused sum:
+// one-sided 650 / 679 / 699 against both-sides 584 / 731 / 746 Gpairs/s at 16384 / 24576 /
+// 32768 particles.
+std::atomic<int64_t> g_sym_min_n{24576};
 
 struct DevInfo {
   int sms = 0;
