@@ -430,7 +430,15 @@ struct RotSweep {
     return VPM_OK;
   }
 
-  // eff_out: the fraction of whole waves the chosen launches fill
+  // Waves (rounds of resident CTAs, each about one tile pair long) that the diagonal-pair
+  // launches of a plan with m pairs per launch take: npairs / m launches of m nt CTAs and a
+  // last one of the remaining pairs.
+  static int64_t pair_waves(int64_t npairs, int64_t nt, int64_t m, int64_t slots) {
+    const int64_t full = npairs / m, rem = npairs - full * m;
+    return full * ((m * nt + slots - 1) / slots) + (rem * nt + slots - 1) / slots;
+  }
+
+  // eff_out: the fraction of whole waves the chosen launches fill (ideal waves / waves)
   static int plan(int64_t n, Plan* p, size_t max_partial_bytes, double* eff_out = nullptr) {
     DevInfo d;
     int rc = device_info(&d);
@@ -440,21 +448,40 @@ struct RotSweep {
     if (rc) return rc;
     const int64_t nt = tiles(n);
     const int64_t npairs = nt / 2;
-    const double slots = double(d.sms) * occ;
-    // pairs per launch: the first m (from 1) whose m * nt CTAs fill 97 % of whole waves,
-    // else the best one up to kMaxPairs
-    int best_m = 1;
-    double best = -1.0;
+    const int64_t slots = int64_t(d.sms) * occ;
+    // Pairs per launch, two candidates within the caller's workspace budget: m0, the first m
+    // whose own launch fills 97 % of whole waves (else the best such fill), and m1, the m whose
+    // launches take the fewest waves in all (the smaller m on a tie).  m0 is kept unless m1
+    // saves more than 1 % of the waves: at equal wave counts the launches of m0 measured up to
+    // 5 % faster (fused sum at 65536, LES sums at 262144), while m1 gains 1.5 % at 2^20 and 7 %
+    // at 49152.
+    int m0 = 1;
+    double be = -1.0;
     for (int m = 1; m <= kMaxPairs && m <= npairs; ++m) {
       if (m > 1 && sets(m) * set_bytes(n) > max_partial_bytes) break;
-      const double waves = double(m) * nt / slots;
+      const double waves = double(m) * nt / double(slots);
       const double eff = waves / std::ceil(waves);
-      if (eff > best + 1e-9) {
-        best = eff;
-        best_m = m;
+      if (eff > be + 1e-9) {
+        be = eff;
+        m0 = m;
       }
       if (eff >= 0.97) break;
     }
+    int m1 = 1;
+    int64_t w1 = pair_waves(npairs, nt, 1, slots);
+    for (int m = 2; m <= kMaxPairs && m <= npairs; ++m) {
+      if (sets(m) * set_bytes(n) > max_partial_bytes) break;
+      const int64_t w = pair_waves(npairs, nt, m, slots);
+      if (w < w1) {
+        w1 = w;
+        m1 = m;
+      }
+    }
+    const int64_t w0 = pair_waves(npairs, nt, m0, slots);
+    const bool keep0 = double(w0) <= 1.01 * double(w1);
+    const int best_m = keep0 ? m0 : m1;
+    const int64_t best_w = keep0 ? w0 : w1;
+    const double best = double(npairs) * nt / double(slots) / double(best_w);
     if (eff_out) *eff_out = best;
     p->pairs = best_m;
     p->tblocks = nt;
