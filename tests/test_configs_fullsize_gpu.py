@@ -13,7 +13,8 @@
   RK4 at dt = 0.002: one step in FP32c and in FP64.  The FP32c sums of the stepped state
   against FP64 (velocity, vorticity and enstrophy 1e-6, stretching 2e-6), the dynamic
   coefficient C_nu of the two runs, and the FP64 LES step sums of the initial state against
-  the oracle on windows of targets at the start, middle and end of the 2^20 rows.
+  the oracle on windows of targets at the start, middle and end of the 2^20 rows (1e-12; the
+  vorticity 3e-12).
 
 The reference's vpmModule.py step (:522-560) and strength update with the LES coefficient
 (:713-884, :887-962) are what the ParticleSystem steps restate."""
@@ -28,7 +29,11 @@ pytestmark = pytest.mark.gpu
 
 VEL_TOL = 1e-6       # FP32c velocity (and vorticity, enstrophy) against FP64
 STRETCH_TOL = 2e-6   # FP32c stretching against FP64 on ring-shaped fields
-FP64_TOL_2_20 = 1e-11  # FP64 against the oracle at 2^20 sources (see test_fullsize_gpu)
+# FP64 against the oracle at 2^20 sources: velocity and stretching at the reference's 1e-12;
+# the particle vorticity (a 2^20-term sum of the zeta kernel with strongly cancelling
+# near-neighbour terms on the ring) measured up to 1.2e-12 on these windows
+FP64_TOL_2_20 = 1e-12
+FP64_TOL_2_20_VORTICITY = 3e-12
 
 
 def _system(tmp_path, name, precision, **cfg):
@@ -199,4 +204,5 @@ def test_les_ring_2e20_sums_vs_oracle_windows():
                                                f.radii)
         es = [normwise(u[t0:t1], ru), normwise(g[t0:t1], rg), normwise(w[t0:t1], rw)]
         print(f"window [{t0}, {t1}): " + ", ".join(f"{e:.2e}" for e in es))
-        assert max(es) <= FP64_TOL_2_20, (t0, es)
+        assert max(es[:2]) <= FP64_TOL_2_20, (t0, es)
+        assert es[2] <= FP64_TOL_2_20_VORTICITY, (t0, es)
