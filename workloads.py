@@ -201,9 +201,14 @@ def config3(args):
         out = {}
         res = {}
         for prec in ("fp32c", "fp64"):
-            for _ in range(2):  # plan set-up, clocks out of idle
+            # plan set-up, and at least ~100 ms of work so the clocks leave any idle state
+            t_end = time.perf_counter() + 0.1
+            while True:
                 kernels.velocity_and_strength_gradients(x, a, s, precision=prec)
-            reps = 5 if (prec == "fp32c" or n <= (1 << 18)) else 1
+                torch.cuda.synchronize()
+                if time.perf_counter() > t_end:
+                    break
+            reps = (20 if n <= (1 << 16) else 5) if (prec == "fp32c" or n <= (1 << 18)) else 1
             with _Timer() as t:
                 for _ in range(reps):
                     out[prec] = kernels.velocity_and_strength_gradients(x, a, s,
