@@ -209,11 +209,14 @@ def config3(args):
                 if time.perf_counter() > t_end:
                     break
             reps = (20 if n <= (1 << 16) else 5) if (prec == "fp32c" or n <= (1 << 18)) else 1
-            with _Timer() as t:
-                for _ in range(reps):
-                    out[prec] = kernels.velocity_and_strength_gradients(x, a, s,
-                                                                        precision=prec)
-            res[prec] = n * n / (t.ms / reps / 1e3) / 1e9
+            best = float("inf")
+            for _ in range(3 if reps > 1 else 1):  # best of three timing windows
+                with _Timer() as t:
+                    for _ in range(reps):
+                        out[prec] = kernels.velocity_and_strength_gradients(x, a, s,
+                                                                            precision=prec)
+                best = min(best, t.ms / reps)
+            res[prec] = n * n / (best / 1e3) / 1e9
         path = ("both-sides" if kernels.sweep_launches("velocity_and_strength_gradients",
                                                         "fp32c", n, n) > 2 else "one-sided")
         ops, rsq = _FUSED_OPS[path]
