@@ -68,7 +68,8 @@ enum vpm_op {
   VPM_OP_RHS_VJP = 9,             /* adjoint of (velocity, stretching) */
   VPM_OP_RHS_VJP_PSE = 10,        /* adjoint of (velocity, stretching + PSE) */
   VPM_OP_KINETIC_ENERGY_GRAD = 11, /* gradient of the kinetic energy */
-  VPM_OP_LES_STEP_SUMS = 12        /* velocity, stretching, vorticity, enstrophy in one sweep */
+  VPM_OP_LES_STEP_SUMS = 12,       /* velocity, stretching, vorticity, enstrophy in one sweep */
+  VPM_OP_LES_TEST_FILTER = 13      /* test-filter sums of the least-squares LES coefficient */
 };
 
 /* ---- library information ------------------------------------------------------------ */
@@ -243,10 +244,19 @@ int vpm_les_update(const double* vorticity, const double* radii, const double* e
  *   Cnu = clip(sqrt(sum L M / sum M M), 1e-9, 0.0761)  (unchanged when either sum is <= 0).
  * vpm_les_lsq_weights writes the per-particle fields the test filter acts on, times the particle
  * volume |alpha|/|w|: weights (n,3) = (|u|^2 v, sigma^2 |w|^2 v, 0).  The caller forms, with the
- * pair-sum entry points and radii 2 sigma: hat u = vpm_selfinduced_velocity, hat w =
- * vpm_vorticity_field_at(x, x, alpha, 2 sigma), hat f = vpm_vorticity_field_at(x, x, weights,
- * 2 sigma).  vpm_les_lsq_update reduces both sums in one block in a fixed order, writes them to
+ * pair-sum entry points and radii 2 sigma: hat u = vpm_selfinduced_velocity, and hat w with
+ * hat f from one vpm_les_test_filter sweep (equal to vpm_vorticity_field_at(x, x, alpha,
+ * 2 sigma) and vpm_vorticity_field_at(x, x, weights, 2 sigma)).  vpm_les_lsq_update reduces both sums in one block in a fixed order, writes them to
  * `sums` (2 device doubles, may be NULL) and updates les_state[0] (= Cnu) on the device. */
+/* The two test-filter sums of the least-squares coefficient in one sweep (no counterpart in
+ * the reference): the vorticity filter sum of vpm_vorticity_field_at(x, x, alpha, test_radii)
+ * into test_vorticity (n,3), and the same filter applied to the first two columns of `fields`
+ * (n,3; the weights of vpm_les_lsq_weights) into test_filtered (n,3, third column 0).
+ * Workspace: vpm_workspace_bytes(VPM_OP_LES_TEST_FILTER, precision, n, n). */
+int vpm_les_test_filter(const double* positions, const double* strengths,
+                        const double* test_radii, const double* fields, int64_t n,
+                        double* test_vorticity, double* test_filtered, int precision,
+                        void* workspace, size_t workspace_bytes, void* stream);
 int vpm_les_lsq_weights(const double* velocities, const double* vorticity,
                         const double* strengths, const double* radii, int64_t n,
                         double* weights, void* stream);

@@ -35,6 +35,7 @@ OPS = {
     "rhs_vjp_pse": 10,
     "kinetic_energy_grad": 11,
     "les_step_sums": 12,
+    "les_test_filter": 13,
 }
 
 _P = ctypes.c_void_p
@@ -78,6 +79,7 @@ SIGNATURES = {
     "vpm_core_spreading": ([_P, _P, _P, _I64, ctypes.c_double, ctypes.c_double, _P], _I),
     "vpm_les_workspace_bytes": ([_I64], _SZ),
     "vpm_les_update": ([_P, _P, _P, _I64, _I, _P, _P, _P, _P, _SZ, _P], _I),
+    "vpm_les_test_filter": ([_P, _P, _P, _P, _I64, _P, _P, _I, _P, _SZ, _P], _I),
     "vpm_les_lsq_weights": ([_P, _P, _P, _P, _I64, _P, _P], _I),
     "vpm_les_lsq_update": ([_P, _P, _P, _P, _I64, _P, _P, _P], _I),
     "vpm_relax_strengths": ([_P, _P, _I64, ctypes.c_double, _P], _I),

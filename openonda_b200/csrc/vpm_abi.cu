@@ -703,6 +703,8 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
       return Sweep<typename O::RhsVjpPse, T>::plan(m, n, p, mpb);
     case VPM_OP_KINETIC_ENERGY_GRAD:
       return Sweep<typename O::KeGrad, T>::plan(m, n, p, mpb);
+    case VPM_OP_LES_TEST_FILTER:
+      return Sweep<OpTestFilter<T, REFINE>, T>::plan(m, n, p, mpb);
     default:
       return fail(VPM_ERR_ARG, "unknown op " + std::to_string(op));
   }
@@ -714,7 +716,9 @@ struct Layout {
 
 template <class T>
 size_t op_record_bytes(int op) {
-  return (op == VPM_OP_RHS_VJP || op == VPM_OP_RHS_VJP_PSE) ? sizeof(RecG<T>) : sizeof(Rec<T>);
+  if (op == VPM_OP_RHS_VJP || op == VPM_OP_RHS_VJP_PSE) return sizeof(RecG<T>);
+  if (op == VPM_OP_LES_TEST_FILTER) return sizeof(RecF<T>);
+  return sizeof(Rec<T>);
 }
 
 template <class T>
@@ -759,6 +763,7 @@ struct Call {
   size_t max_partial_bytes = kMaxPartialBytes;  // caps the source splits of the plan
   double* out3 = nullptr;  // VPM_OP_LES_STEP_SUMS: vorticity (m,3)
   double* out4 = nullptr;  // VPM_OP_LES_STEP_SUMS: enstrophy (device scalar)
+  const double* aux = nullptr;  // VPM_OP_LES_TEST_FILTER: the filtered fields (n,3)
 };
 
 template <class T, bool REFINE, bool UC>
@@ -904,6 +909,75 @@ int run(const Call& c) {
     default:
       return fail(VPM_ERR_ARG, "unknown op " + std::to_string(c.op));
   }
+}
+
+// ---- LES test filter (least-squares dynamic coefficient) ----------------------------------
+template <class E>
+__global__ void pack_filter_kernel(const double* __restrict__ pos, const double* __restrict__ str,
+                                   const double* __restrict__ rad, const double* __restrict__ f,
+                                   int64_t n, RecF<E>* __restrict__ out) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  RecF<E> r;
+  set_elem(r.x, pos[3 * i]);
+  set_elem(r.y, pos[3 * i + 1]);
+  set_elem(r.z, pos[3 * i + 2]);
+  set_elem(r.s, rad[i]);
+  set_elem(r.ax, str[3 * i]);
+  set_elem(r.ay, str[3 * i + 1]);
+  set_elem(r.az, str[3 * i + 2]);
+  set_elem(r.f1, f[3 * i]);
+  set_elem(r.f2, f[3 * i + 1]);
+  set_elem(r.pad, 0.0);
+  out[i] = r;
+}
+
+// w_hat (m,3) and the two filtered fields (m,3; third column 0), both with the zeta kernel's
+// 7.5/(4 pi) as in vpm_vorticity_field_at.
+template <class T>
+__global__ void finalize_filter_kernel(const double* __restrict__ part, int splits, int64_t m,
+                                       double* __restrict__ w_hat, double* __restrict__ f_hat) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double v[5];
+  sum_splits<5>(part, splits, m, i, v);
+  const double c = 7.5 * kOneOver4Pi;
+  w_hat[3 * i] = v[0] * c;
+  w_hat[3 * i + 1] = v[1] * c;
+  w_hat[3 * i + 2] = v[2] * c;
+  f_hat[3 * i] = v[3] * c;
+  f_hat[3 * i + 1] = v[4] * c;
+  f_hat[3 * i + 2] = 0.0;
+}
+
+template <class T, bool REFINE>
+int run_filter(const Call& c) {
+  using Op = OpTestFilter<T, REFINE>;
+  int rc = check_arch();
+  if (rc) return rc;
+  if (c.n == 0) return VPM_OK;
+  Plan p;
+  Layout L;
+  rc = workspace_for<T, REFINE>(c.op, c.n, c.n, &L, &p, c.max_partial_bytes);
+  if (rc) return rc;
+  if (c.ws == nullptr) return fail(VPM_ERR_WORKSPACE, "workspace is null");
+  if (reinterpret_cast<uintptr_t>(c.ws) % kAlign != 0)
+    return fail(VPM_ERR_ALIGN, "workspace must be 256-byte aligned");
+  if (c.ws_bytes < L.total)
+    return fail(VPM_ERR_WORKSPACE, "workspace has " + std::to_string(c.ws_bytes) +
+                                       " bytes, needs " + std::to_string(L.total));
+  char* ws = static_cast<char*>(c.ws);
+  RecF<T>* rec = reinterpret_cast<RecF<T>*>(ws + L.src_off);
+  double* part = reinterpret_cast<double*>(ws + L.part_off);
+  const unsigned blocks = unsigned((c.n + 255) / 256);
+  pack_filter_kernel<T><<<blocks, 256, 0, c.st>>>(c.pos, c.str, c.rad, c.aux, c.n, rec);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "pack launch");
+  rc = Sweep<Op, T>::launch(p, rec, c.n, 0, rec, c.n, part, c.st);
+  if (rc) return rc;
+  finalize_filter_kernel<T><<<blocks, 256, 0, c.st>>>(part, p.splits, c.n, c.out, c.out2);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? VPM_OK : cuda_fail(e, "finalize launch");
 }
 
 // Decoded precision code: compute type, Newton-refined rsqrt, uniform cores.
@@ -1385,6 +1459,30 @@ int vpm_les_step_sums(const double* positions, const double* strengths, const do
   c.out3 = vorticity;
   c.out4 = enstrophy;
   return dispatch(c, precision);
+}
+
+int vpm_les_test_filter(const double* positions, const double* strengths,
+                        const double* test_radii, const double* fields, int64_t n,
+                        double* test_vorticity, double* test_filtered, int precision,
+                        void* workspace, size_t workspace_bytes, void* stream) {
+  if (n < 0) return fail(VPM_ERR_ARG, "negative size");
+  if (n > 0 && (!positions || !strengths || !test_radii || !fields || !test_vorticity ||
+                !test_filtered))
+    return fail(VPM_ERR_ARG, "null pointer");
+  Call c{VPM_OP_LES_TEST_FILTER, nullptr, n, positions, strengths, test_radii, nullptr, n,
+         test_vorticity, test_filtered, 0, workspace, workspace_bytes,
+         static_cast<cudaStream_t>(stream)};
+  c.aux = fields;
+  switch (precision & ~VPM_UNIFORM_CORE) {
+    case VPM_FP64:
+      return run_filter<double, false>(c);
+    case VPM_FP32C:
+      return run_filter<float2, false>(c);
+    case VPM_FP32C_REFINED:
+      return run_filter<float2, true>(c);
+    default:
+      return fail(VPM_ERR_ARG, "unknown precision " + std::to_string(precision));
+  }
 }
 
 size_t vpm_record_bytes(int precision) {

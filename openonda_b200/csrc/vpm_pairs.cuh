@@ -188,6 +188,77 @@ struct OpVortAt : PairOpBase<V> {
   }
 };
 
+// ---- LES test filter: the vorticity filter sum with two more particle fields -------------
+// The least-squares dynamic coefficient needs, at the test-filter width, the vorticity and
+// the filtered fields (|u|^2 v, sigma^2 |w|^2 v): one probe-style sweep of the particles over
+// themselves with the zeta kernel of the source core (here 2 sigma_j), pairs with
+// r^2 <= 1e-8 skipped as in OpVortAt.  Record: position, core, strength and the two fields,
+// 80 bytes in both precisions.
+template <class E>
+struct alignas(16) RecF {
+  E x, y, z, s;
+  E ax, ay, az, f1;
+  E f2, pad;
+};
+static_assert(sizeof(RecF<double>) == 80 && sizeof(RecF<float2>) == 80, "RecF is 80 B");
+
+template <class V>
+struct SrcF {
+  V x, y, z, s, ax, ay, az, f1, f2;
+};
+template <class V>
+struct TgtF {
+  V x, y, z;
+};
+
+__device__ __forceinline__ SrcF<double> load_srcf(const RecF<double>& r) {
+  const double2* p = reinterpret_cast<const double2*>(&r);
+  const double2 a = p[0], b = p[1], c = p[2], d = p[3], e = p[4];
+  return SrcF<double>{a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x};
+}
+__device__ __forceinline__ SrcF<float2> load_srcf(const RecF<float2>& r) {
+  const float4* p = reinterpret_cast<const float4*>(&r);
+  const float4 a = p[0], b = p[1], c = p[2], d = p[3], e = p[4];
+  return SrcF<float2>{make_float2(a.x, a.y), make_float2(a.z, a.w), make_float2(b.x, b.y),
+                      make_float2(b.z, b.w), make_float2(c.x, c.y), make_float2(c.z, c.w),
+                      make_float2(d.x, d.y), make_float2(d.z, d.w), make_float2(e.x, e.y)};
+}
+__device__ __forceinline__ TgtF<double> make_tgtf(const RecF<double>* const* r) {
+  return TgtF<double>{r[0]->x, r[0]->y, r[0]->z};
+}
+__device__ __forceinline__ TgtF<float2> make_tgtf(const RecF<float2>* const* r) {
+  return TgtF<float2>{make_float2(r[0]->x.x, r[1]->x.x), make_float2(r[0]->y.x, r[1]->y.x),
+                      make_float2(r[0]->z.x, r[1]->z.x)};
+}
+
+template <class V, bool REFINE>
+struct OpTestFilter {
+  static constexpr int NV = 5;
+  static constexpr int kR = 0;
+  static constexpr int kWindow = 0;
+  using Record = RecF<V>;
+  using SrcT = SrcF<V>;
+  using TgtT = TgtF<V>;
+  __device__ __forceinline__ static SrcT load(const Record& r) { return load_srcf(r); }
+  __device__ __forceinline__ static TgtT target(const Record* const* r) { return make_tgtf(r); }
+  __device__ __forceinline__ static void pair(const TgtT& t, V* acc, const SrcT& s,
+                                              const int64_t*, int64_t) {
+    const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
+    const V r2 = fma(rx, rx, fma(ry, ry, rz * rz));
+    const V s2 = s.s * s.s;
+    const V y = rsqrt_lane<REFINE>(r2 + s2);
+    const V y2 = y * y;
+    const V y3 = y2 * y;
+    const V y7 = (y3 * y3) * y;
+    const V k = (s2 * s2) * y7;
+    acc[0] = fma_if_gt(r2, kRefEps, k, s.ax, acc[0]);
+    acc[1] = fma_if_gt(r2, kRefEps, k, s.ay, acc[1]);
+    acc[2] = fma_if_gt(r2, kRefEps, k, s.az, acc[2]);
+    acc[3] = fma_if_gt(r2, kRefEps, k, s.f1, acc[3]);
+    acc[4] = fma_if_gt(r2, kRefEps, k, s.f2, acc[4]);
+  }
+};
+
 // ---- stretching (transpose scheme): A += g (a_j - a_i),  B += f (r . (d x a_i)) r -------
 template <class V, bool REFINE, bool UC = false>
 struct OpStretch : PairOpBase<V> {

@@ -162,6 +162,22 @@ def les_step_sums(positions, strengths, radii, ref_extra_4pi=True,
     return u, g, w, e
 
 
+def les_test_filter(positions, strengths, test_radii, fields, precision="fp64"):
+    """The two test-filter sums of the least-squares LES coefficient in one sweep: the
+    vorticity filter sum with cores ``test_radii`` and the same filter applied to the first two
+    columns of ``fields`` (n, 3).  Returns (test_vorticity, test_filtered), both (n, 3)."""
+    x, a, s, n, dev = _self_inputs(positions, strengths, test_radii)
+    f = _check_vec("fields", fields, n)
+    _same_device(x, f)
+    w = torch.empty((n, 3), dtype=_F64, device=dev)
+    fh = torch.empty((n, 3), dtype=_F64, device=dev)
+    ws, nb = _workspace("les_test_filter", precision, n, n, dev)
+    _lib.check(_lib.load().vpm_les_test_filter(
+        _ptr(x), _ptr(a), _ptr(s), _ptr(f), n, _ptr(w), _ptr(fh),
+        _lib.precision_code(precision), _ptr(ws), ws.numel(), _stream(dev)))
+    return w, fh
+
+
 def strength_gradients_pse(positions, strengths, radii, viscosities,
                            precision="fp64", uniform_core=False):
     x, a, s, n, dev = _self_inputs(positions, strengths, radii)

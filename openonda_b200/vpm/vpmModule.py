@@ -821,9 +821,10 @@ class ParticleSystem:
     def _les_least_squares(self, vorticity, velocities=None):
         """Cnu from the Germano identity for the sub-filter kinetic energy between the particle
         filter (core sigma) and a test filter of core 2 sigma, by least squares over all
-        particles in FP64 (vpm_les_lsq_update).  Three extra sweeps: the test-filtered
-        velocity, vorticity and the test filter of (|u|^2, sigma^2 |w|^2) times the particle
-        volume.  Returns the device sums (sum L M, sum M M)."""
+        particles in FP64 (vpm_les_lsq_update).  Two extra sweeps: the test-filtered velocity,
+        and one sweep for the test-filtered vorticity together with the test filter of
+        (|u|^2, sigma^2 |w|^2) times the particle volume.  Returns the device sums
+        (sum L M, sum M M)."""
         dev = self._dev()
         lib = _lib.load()
         st = _stream(dev)
@@ -831,11 +832,10 @@ class ParticleSystem:
         s2 = 2.0 * self._s
         uh = kernels.selfinduced_velocity(self._x, self._a, s2, precision=self.precision,
                                           uniform_core=self._uc)
-        wh = kernels.vorticity_field_at(self._x, self._x, self._a, s2, precision=self.precision)
         wts = torch.empty_like(self._a)
         _check(lib.vpm_les_lsq_weights(u.data_ptr(), vorticity.data_ptr(), self._a.data_ptr(),
                                        self._s.data_ptr(), self._n, wts.data_ptr(), st))
-        fh = kernels.vorticity_field_at(self._x, self._x, wts, s2, precision=self.precision)
+        wh, fh = kernels.les_test_filter(self._x, self._a, s2, wts, precision=self.precision)
         sums = torch.empty(2, dtype=_F64, device=dev)
         _check(lib.vpm_les_lsq_update(uh.data_ptr(), wh.data_ptr(), fh.data_ptr(),
                                       self._s.data_ptr(), self._n, self._les_state().data_ptr(),

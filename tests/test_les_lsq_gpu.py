@@ -81,3 +81,30 @@ def test_lsq_step_graph_equals_eager_and_stays_in_range(tmp_path):
     from openonda_b200 import kernels
 
     assert kernels.device_errors() == 0
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("fp32c", 1e-6)])
+def test_test_filter_sweep_equals_two_vorticity_sums(precision, tol):
+    """vpm_les_test_filter (one sweep, 80-byte records) against two vpm_vorticity_field_at
+    sweeps with the same cores and strengths."""
+    from openonda_b200 import configs, kernels
+
+    f = configs.random_cloud(3000, seed=13)
+    f.radii *= 4
+    rng = np.random.default_rng(13)
+    fields = np.zeros((f.n, 3))
+    fields[:, :2] = rng.uniform(0.0, 1e-3, size=(f.n, 2))
+    r = (lambda z: np.asarray(z, np.float32).astype(np.float64)) if precision != "fp64" \
+        else np.asarray
+    x, a, s, fl = (torch.from_numpy(np.ascontiguousarray(r(z))).cuda()
+                   for z in (f.positions, f.strengths, 2.0 * f.radii, fields))
+    wh, fh = kernels.les_test_filter(x, a, s, fl, precision=precision)
+    wref = kernels.vorticity_field_at(x, x, a, s, precision="fp64")
+    fref = kernels.vorticity_field_at(x, x, fl, s, precision="fp64")
+    ew = float((wh - wref).abs().max() / wref.abs().max())
+    ef = float((fh[:, :2] - fref[:, :2]).abs().max() / fref[:, :2].abs().max())
+    print(f"{precision}: test vorticity {ew:.2e}, filtered fields {ef:.2e}")
+    assert ew <= tol and ef <= tol
+    assert float(fh[:, 2].abs().max()) == 0.0
+    assert kernels.device_errors() == 0
+

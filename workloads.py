@@ -354,6 +354,7 @@ def sweeps(args):
             lambda uc: kernels.velocity_and_strength_gradients(x, a, s, precision=p,
                                                                uniform_core=uc),
         "vorticity_field_at": lambda uc: kernels.vorticity_field_at(x, x, a, s, precision=p),
+        "les_test_filter": lambda uc: kernels.les_test_filter(x, a, 2.0 * s, a, precision=p),
         "total_enstrophy": lambda uc: kernels.total_enstrophy(x, a, s, precision=p,
                                                               uniform_core=uc),
         "strength_gradients_pse":
@@ -365,8 +366,8 @@ def sweeps(args):
     reps = args.steps or 3
     for name, fn in cases.items():
         for uc in (False, True):
-            if uc and name == "vorticity_field_at":
-                continue  # probe sums have no uniform-core form
+            if uc and name in ("vorticity_field_at", "les_test_filter"):
+                continue  # probe-style sums have no uniform-core form
             fn(uc)
             with _Timer() as t:
                 for _ in range(reps):
