@@ -354,6 +354,28 @@ finalize_dot_kernel(const double* __restrict__ part, int splits, int64_t m,
   if (threadIdx.x == 0) out[0] = red[0] * scale;
 }
 
+// scale * the sum over all targets of value OFF of NV partial sums per target, in a fixed
+// order (the same one as finalize_dot_kernel)
+template <int NV, int OFF>
+__global__ void __launch_bounds__(kReduceThreads)
+finalize_sum_kernel(const double* __restrict__ part, int splits, int64_t m, double scale,
+                    double* __restrict__ out) {
+  __shared__ double red[kReduceThreads];
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < m; i += kReduceThreads) {
+    double v = 0.0;
+    for (int s = 0; s < splits; ++s) v += part[(int64_t(s) * NV + OFF) * m + i];
+    acc += v;
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = kReduceThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = red[0] * scale;
+}
+
 __global__ void write_scalar_kernel(double* out, double v) { out[0] = v; }
 
 template <class T, int KIND, int NV>
@@ -871,16 +893,25 @@ int run(const Call& c) {
           rc = RotSweep<typename O::LesStepBoth>::launch(p, src, c.n, part, c.st);
       }
       if (!p.pairs) rc = Sweep<Op, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
-      if (!rc)
-        rc = finalize_vec<T, FIN_LES, Op::NV>(part, p.splits, c.m, tgt, c.out, c.out2, c.st,
-                                               c.out3);
       if (rc) return rc;
       double scale = 1.0 / (8.0 * kPi);
       if (c.ref_extra_4pi) scale /= 4.0 * kPi;
-      // the both-sides sweep sums the symmetric enstrophy term once per unordered pair
-      if (p.pairs) scale *= 2.0;
-      finalize_dot_kernel<T, Op::NV, 12><<<1, kReduceThreads, 0, c.st>>>(part, p.splits, c.m,
-                                                                          tgt, scale, c.out4);
+      if (p.pairs) {
+        // both sides: the per-target scalar sum_j ke (a_i . a_j) (value 12), taken once per
+        // unordered pair, so the sum is doubled
+        constexpr int NVB = O::LesStepBoth::NV;
+        rc = finalize_vec<T, FIN_LES, NVB>(part, p.splits, c.m, tgt, c.out, c.out2, c.st,
+                                           c.out3);
+        if (rc) return rc;
+        finalize_sum_kernel<NVB, 12><<<1, kReduceThreads, 0, c.st>>>(part, p.splits, c.m,
+                                                                     2.0 * scale, c.out4);
+      } else {
+        rc = finalize_vec<T, FIN_LES, Op::NV>(part, p.splits, c.m, tgt, c.out, c.out2, c.st,
+                                               c.out3);
+        if (rc) return rc;
+        finalize_dot_kernel<T, Op::NV, 12><<<1, kReduceThreads, 0, c.st>>>(part, p.splits, c.m,
+                                                                            tgt, scale, c.out4);
+      }
       cudaError_t e = cudaGetLastError();
       return e == cudaSuccess ? VPM_OK : cuda_fail(e, "reduce launch");
     }

@@ -133,6 +133,21 @@ __host__ __device__ constexpr int rot_tile() {
 #ifndef VPM_ROT_TGT_WINDOW
 #define VPM_ROT_TGT_WINDOW 32
 #endif
+// Target-side windows per value in the fused and LES operators.  The stretching term
+// g (a_j - a_i) (values 3-5) has the FP32 partial sums that cancel most: its error sets the
+// stretching error and grows with the window, so it folds every 16 steps.  The other values
+// (velocity, the stretching term f (r . (a_i x (r x a_j))) r, vorticity, the enstrophy filter
+// sum) fold every 64 steps, so a 64-step span has as many folds as with 32-step windows for
+// all.  On the leapfrogging rings (N = 131072, 50 steps) the stretching error went from
+// 1.5-1.9e-6 to 0.9-1.2e-6 and the velocity error from 0.8-0.9e-7 to 1.2-1.4e-7, at the
+// same sweep time; on the dynamic-LES ring (N = 2^20) the LES step's stretching error from
+// 1.65e-6 to 1.48e-6 and its vorticity error from 2.9e-7 to 3.8e-7.
+#ifndef VPM_ROT_STRETCH_TGT_WINDOW
+#define VPM_ROT_STRETCH_TGT_WINDOW 16
+#endif
+#ifndef VPM_ROT_LONG_TGT_WINDOW
+#define VPM_ROT_LONG_TGT_WINDOW 64
+#endif
 
 // Dynamic shared memory of one CTA: the target-side FP64 carries [NV][T], then the
 // source-side sums of the first kSymFrom values, [kJBufs][kSymFrom][warps * 32].
@@ -185,6 +200,16 @@ struct RotStd {
                 make_float2(c.az, c.az), make_float2(0.f, 0.f)};
   }
   __device__ __forceinline__ static TgtT target(const Record* const* r) { return make_tgt(r); }
+  // Uniform cores: every record carries the same core, so the target's core, core^2 and
+  // core^4 come from one record for all of a thread's packed lanes (one register pair each
+  // instead of one per lane; the values are the same bits as the lanes' own)
+  static constexpr bool kUniformCore = UC;
+  __device__ __forceinline__ static void uniform_core(TgtT& t, const Record* rec) {
+    const float sc = rec[0].s.x, s2 = sc * sc;
+    t.sc = make_float2(sc, sc);
+    t.s2c = make_float2(s2, s2);
+    t.s4c = make_float2(s2 * s2, s2 * s2);
+  }
   // one-sided pair of the diagonal tiles; these operators need no index for the pair i == j
   // (it adds nothing, except the enstrophy filter sum, which includes it as the reference does)
   __device__ __forceinline__ static void diag(const TgtT& t, V* acc, const SrcT& s,
@@ -193,6 +218,12 @@ struct RotStd {
   }
   // every source-side sum is carried and stored
   __device__ __forceinline__ static constexpr bool carried(int) { return true; }
+  // values folded into the FP64 carries every kTgtWindowShort steps instead of every
+  // kTgtWindow (0: none), and values folded every kTgtWindowLong steps (whole batches; 0: none)
+  static constexpr int kTgtWindowShort = 0;
+  __device__ __forceinline__ static constexpr bool short_fold(int) { return false; }
+  static constexpr int kTgtWindowLong = 0;
+  __device__ __forceinline__ static constexpr bool long_fold(int) { return false; }
 };
 
 // Fused velocity + stretching, both sides of the pair (FP32x2 lanes).  Built for 3 and for 2
@@ -206,8 +237,12 @@ struct OpVelStretchBoth : RotStd<OpVelStretch<float2, REFINE, UC>, UC> {
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   static constexpr int kSrcWindow = VPM_ROT_SRC_WINDOW;
   static constexpr int kTgtWindow = VPM_ROT_TGT_WINDOW;
+  static constexpr int kTgtWindowShort = VPM_ROT_STRETCH_TGT_WINDOW;
+  static constexpr int kTgtWindowLong = VPM_ROT_LONG_TGT_WINDOW;
   static constexpr int kSymFrom = NV;  // every sum has a source side
   static constexpr int kJBufs = 2;     // double-buffered source-side sums
+  __device__ __forceinline__ static constexpr bool short_fold(int v) { return v >= 3 && v < 6; }
+  __device__ __forceinline__ static constexpr bool long_fold(int v) { return v < 3 || v >= 6; }
   __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
                                                const Src<V>& s) {
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
@@ -216,10 +251,19 @@ struct OpVelStretchBoth : RotStd<OpVelStretch<float2, REFINE, UC>, UC> {
     const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
     const V y = rsqrt_lane<REFINE>(x);
     const V y2 = y * y;
-    const V y5 = (y2 * y2) * y;
-    const V t1 = fma(splat<V>(1.5), s2, x);
-    const V g = t1 * y5;
-    const V f = (t1 + s2) * (y5 * y2);
+    V g, f;
+    if constexpr (UC) {
+      // (x + 1.5 s^2) y^5 = y^3 (1 + 1.5 s^2 y^2) and (x + 2.5 s^2) y^7 = y^5 (1 + 2.5 s^2 y^2),
+      // with 1.5 s^2 and 2.5 s^2 loop-invariant: one op fewer per pair
+      const V y3 = y2 * y;
+      g = y3 * fma(splat<V>(1.5f) * s2, y2, splat<V>(1.f));
+      f = (y3 * y2) * fma(splat<V>(2.5f) * s2, y2, splat<V>(1.f));
+    } else {
+      const V y5 = (y2 * y2) * y;
+      const V t1 = fma(splat<V>(1.5), s2, x);
+      g = t1 * y5;
+      f = (t1 + s2) * (y5 * y2);
+    }
     const V cx = fma(ry, s.az, -(rz * s.ay));
     const V cy = fma(rz, s.ax, -(rx * s.az));
     const V cz = fma(rx, s.ay, -(ry * s.ax));
@@ -270,8 +314,13 @@ struct OpVelBoth : RotStd<OpVel<float2, REFINE, UC>, UC> {
     const V x = fma(rx, rx, fma(ry, ry, fma(rz, rz, s2)));
     const V y = rsqrt_lane<REFINE>(x);
     const V y2 = y * y;
-    const V y5 = (y2 * y2) * y;
-    const V g = fma(splat<V>(1.5), s2, x) * y5;
+    V g;
+    if constexpr (UC) {
+      g = (y2 * y) * fma(splat<V>(1.5f) * s2, y2, splat<V>(1.f));  // y^3 (1 + 1.5 s^2 y^2)
+    } else {
+      const V y5 = (y2 * y2) * y;
+      g = fma(splat<V>(1.5), s2, x) * y5;
+    }
     const V cx = fma(ry, s.az, -(rz * s.ay));  // r x a_j
     const V cy = fma(rz, s.ax, -(rx * s.az));
     const V cz = fma(rx, s.ay, -(ry * s.ax));
@@ -329,19 +378,26 @@ struct OpPseBoth : RotStd<OpPse<float2, REFINE, UC>, UC> {
 // particle that is summed over, so target i takes s_j^4 (r^2 + s_j^2)^-7/2 a_j and particle
 // j takes s_i^4 (r^2 + s_i^2)^-7/2 a_i (one rsqrt each; with uniform cores both equal the
 // pair core's y and need none); the enstrophy filter sum (x + 2.2 s^2) y^3 is symmetric.
-// Vorticity and enstrophy are symmetric sums, so their source-side terms enter negated (the
-// stored value is negated once more).  Pairs with r^2 <= 1e-8 add no vorticity.  69 FP32
-// lane-ops per unordered pair with uniform cores, about 82 without (one-sided: 2 x 52,
-// 2 x 56).  255 registers per thread: two CTAs per SM, step loop unrolled 2.
+// The vorticity sum is symmetric, so its source-side terms enter negated (the stored value is
+// negated once more).  Pairs with r^2 <= 1e-8 add no vorticity.  Only the scalar
+// sum_i a_i . E_i of the enstrophy filter sum is wanted, so each target carries the one sum
+// sum_j ke (a_i . a_j) (value 12) in place of the three components of E_i.  65 FP32 lane-ops
+// per unordered pair with uniform cores, about 80 without (one-sided: 2 x 52, 2 x 56).  Two
+// CTAs per SM, step loop unrolled 2.
 template <bool REFINE, bool UC>
 struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
   using V = float2;
-  static constexpr int NV = 15;
+  using OneSided = OpLesStep<float2, REFINE, UC>;
+  static constexpr int NV = 13;
   static constexpr int kMinBlocks = VPM_ROT15_MINB;
   static constexpr int kUnroll = VPM_ROT15_UNROLL;
   static constexpr int kSrcWindow = VPM_ROT_SRC_WINDOW;
   static constexpr int kTgtWindow = VPM_ROT_TGT_WINDOW;
-  // values 12-14 (enstrophy filter sum) are taken once per unordered pair, target side only
+  static constexpr int kTgtWindowShort = VPM_ROT_STRETCH_TGT_WINDOW;
+  static constexpr int kTgtWindowLong = VPM_ROT_LONG_TGT_WINDOW;
+  __device__ __forceinline__ static constexpr bool short_fold(int v) { return v >= 3 && v < 6; }
+  __device__ __forceinline__ static constexpr bool long_fold(int v) { return v < 3 || v >= 6; }
+  // value 12 (enstrophy filter sum) is taken once per unordered pair, target side only
   static constexpr int kSymFrom = 12;
   // three resident CTAs fit the shared memory only with one buffer of source-side sums
   static constexpr int kJBufs = VPM_ROT15_MINB >= 3 ? 1 : 2;
@@ -357,9 +413,11 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
     const V y2 = y * y;
     const V y3 = y2 * y;
     const V y5 = y3 * y2;
+    // (the y^3 (1 + 1.5 s^2 y^2) form of the other operators measured slower here)
+    const V y7 = y5 * y2;
     const V t1 = fma(splat<V>(1.5), s2, x);
     const V g = t1 * y5;
-    const V f = (t1 + s2) * (y5 * y2);
+    const V f = (t1 + s2) * y7;
     const V cx = fma(ry, s.az, -(rz * s.ay));  // r x a_j
     const V cy = fma(rz, s.ax, -(rx * s.az));
     const V cz = fma(rx, s.ay, -(ry * s.ax));
@@ -390,7 +448,6 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
     const float eps = float(kRefEps);
     V ki, kj;
     if constexpr (UC) {
-      const V y7 = (y3 * y3) * y;
       ki = t.s4c * y7;
       kj = ki;
     } else {
@@ -412,13 +469,25 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
     jv[9] = fma(-kj, t.ax, jv[9]);
     jv[10] = fma(-kj, t.ay, jv[10]);
     jv[11] = fma(-kj, t.az, jv[11]);
-    // enstrophy filter sum (pair core): only the scalar sum_i a_i . E_i is wanted and the pair
-    // term is symmetric, so target i takes the pair once and the finalize doubles it; particle
-    // j takes nothing (the diagonal tiles, visited one-sided, are folded at half weight)
+    // enstrophy filter sum (pair core): the pair term ke (a_i . a_j) is symmetric, so target
+    // i takes the pair once and the finalize doubles it; particle j takes nothing (the
+    // diagonal tiles, visited one-sided, are folded at half weight)
     const V ke = fma(splat<V>(2.2), s2, x) * y3;
-    acc[12] = fma(ke, s.ax, acc[12]);
-    acc[13] = fma(ke, s.ay, acc[13]);
-    acc[14] = fma(ke, s.az, acc[14]);
+    acc[12] = fma(ke, fma(t.ax, s.ax, fma(t.ay, s.ay, t.az * s.az)), acc[12]);
+  }
+  // one-sided pair of the diagonal tiles: the one-sided operator's 15 sums, its enstrophy
+  // components E_i dotted with a_i into value 12
+  __device__ __forceinline__ static void diag(const Tgt<V>& t, V* acc, const Src<V>& s,
+                                              const int64_t*, int64_t) {
+    V full[OneSided::NV];
+    static_assert(OneSided::NV == 15, "velocity, stretching, vorticity, 3 enstrophy sums");
+#pragma unroll
+    for (int v = 0; v < 12; ++v) full[v] = acc[v];
+    full[12] = full[13] = full[14] = make_float2(0.f, 0.f);
+    OneSided::pair(t, full, s, nullptr, 0);
+#pragma unroll
+    for (int v = 0; v < 12; ++v) acc[v] = full[v];
+    acc[12] = fma(t.ax, full[12], fma(t.ay, full[13], fma(t.az, full[14], acc[12])));
   }
 };
 
@@ -455,8 +524,14 @@ struct OpRhsVjpBoth {
   static constexpr int kUnroll = PSE ? VPM_ROTGP_UNROLL : VPM_ROTG_UNROLL;
   static constexpr int kSrcWindow = VPM_ROTG_SRC_WINDOW;
   static constexpr int kTgtWindow = 32;
+  static constexpr int kTgtWindowShort = 0;
+  __device__ __forceinline__ static constexpr bool short_fold(int) { return false; }
+  static constexpr int kTgtWindowLong = 0;
+  __device__ __forceinline__ static constexpr bool long_fold(int) { return false; }
   static constexpr int kSymFrom = NV;
   static constexpr int kJBufs = 2;
+  static constexpr bool kUniformCore = false;
+  __device__ __forceinline__ static void uniform_core(TgtT&, const Record*) {}
 
   __device__ __forceinline__ static Lane load_lane(const Record* rec, int64_t j, int64_t n) {
     if (j < n) {
@@ -615,6 +690,11 @@ rot_sweep_kernel(const RotArgs a) {
   constexpr int TW = Op::kTgtWindow;
   static_assert(32 % SW == 0, "the source window divides the 32 steps of a batch");
   static_assert(32 % TW == 0 && TW % SW == 0, "target windows are whole source windows");
+  constexpr int TWS = Op::kTgtWindowShort;
+  static_assert(TWS == 0 || (TW % TWS == 0 && TWS % SW == 0),
+                "short target windows divide the target window and are whole source windows");
+  constexpr int TWL = Op::kTgtWindowLong;
+  static_assert(TWL == 0 || TWL % 32 == 0, "long target windows are whole batches");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* car = reinterpret_cast<double*>(smem_raw);  // [NV][T]
   // [2][NV][WT]: each warp's packed source-side sums of the current batch, per source
@@ -669,6 +749,7 @@ rot_sweep_kernel(const RotArgs a) {
     const int64_t t0 = i0 + lt[2 * p], t1 = i0 + lt[2 * p + 1];
     const Record* recs[2] = {rec + (t0 < a.n ? t0 : a.n - 1), rec + (t1 < a.n ? t1 : a.n - 1)};
     tg[p] = Op::target(recs);
+    if constexpr (Op::kUniformCore) Op::uniform_core(tg[p], rec);
   }
   float2 acc[P][NV];
 #pragma unroll
@@ -676,6 +757,28 @@ rot_sweep_kernel(const RotArgs a) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) acc[p][v] = make_float2(0.f, 0.f);
   __syncthreads();  // carries zeroed
+
+  // target side: the FP32 window sums of the values take(v) selects into the FP64 carries
+  // (each thread its own rows), and those sums start again from zero
+  auto fold_targets = [&](auto take) {
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        if (!take(v)) continue;
+        if (DIAG && v >= NJ) {
+          // a symmetric sum taken once per unordered pair elsewhere: the diagonal tiles
+          // visit every ordered pair, so they count half (the finalize doubles the sum)
+          car[v * T + lt[2 * p]] += 0.5 * double(acc[p][v].x);
+          car[v * T + lt[2 * p + 1]] += 0.5 * double(acc[p][v].y);
+        } else {
+          car[v * T + lt[2 * p]] += double(acc[p][v].x);
+          car[v * T + lt[2 * p + 1]] += double(acc[p][v].y);
+        }
+        acc[p][v] = make_float2(0.f, 0.f);
+      }
+    }
+  };
 
   const int nb = (cnt + 31) / 32;
   Lane nxt = Op::load_lane(rec, j0 + lane, j0 + cnt);
@@ -731,25 +834,16 @@ rot_sweep_kernel(const RotArgs a) {
           }
         }
       }
-      if (((w + 1) * SW) % TW == 0) {
-        // target side: the window's FP32 sums into the FP64 carries (each thread its own rows)
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-#pragma unroll
-          for (int v = 0; v < NV; ++v) {
-            if (DIAG && v >= NJ) {
-              // a symmetric sum taken once per unordered pair elsewhere: the diagonal tiles
-              // visit every ordered pair, so they count half (the finalize doubles the sum)
-              car[v * T + lt[2 * p]] += 0.5 * double(acc[p][v].x);
-              car[v * T + lt[2 * p + 1]] += 0.5 * double(acc[p][v].y);
-            } else {
-              car[v * T + lt[2 * p]] += double(acc[p][v].x);
-              car[v * T + lt[2 * p + 1]] += double(acc[p][v].y);
-            }
-            acc[p][v] = make_float2(0.f, 0.f);
-          }
-        }
-      }
+      const int done = (w + 1) * SW;  // steps of this batch done
+      const bool at_full = done % TW == 0;
+      const bool at_short = TWS > 0 && done % (TWS > 0 ? TWS : 1) == 0;
+      const bool at_long = TWL > 0 && (b * 32 + done) % (TWL > 0 ? TWL : 1) == 0;
+      if (at_full || at_short || at_long)
+        fold_targets([&](int v) {
+          return (TWL > 0 && Op::long_fold(v))    ? at_long
+                 : (TWS > 0 && Op::short_fold(v)) ? at_short
+                                                  : at_full;
+        });
     }
     if constexpr (!DIAG) {
       __syncthreads();  // the batch's source-side sums are complete
@@ -773,6 +867,8 @@ rot_sweep_kernel(const RotArgs a) {
       if constexpr (Op::kJBufs == 1) __syncthreads();
     }
   }
+  // long windows span batches: what the last one left
+  if constexpr (TWL > 0) fold_targets([](int v) { return Op::long_fold(v); });
   __syncthreads();
   for (int q = tid; q < T * NV; q += kRotThreads) {
     const int v = q / T, t = q - v * T;
