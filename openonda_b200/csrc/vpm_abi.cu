@@ -91,12 +91,16 @@ struct Plan {
   int nv = 0;
   int pairs = 0;  // both-sides sweep (vpm_rot.cuh): diagonal pairs per launch; 0 = one-sided
   int variant = 0;  // both-sides fused sum: 0 = built for VPM_ROT_MINB CTAs/SM, 1 = _ALT
+  // both-sides sweep: the diagonal tiles run beside the (single) diagonal-pair launch on a
+  // second stream, into their own accumulator sets after the pairs' ones
+  int diag_beside = 0;
 };
 
 // FP32 self sums with at least this many particles evaluate each unordered pair once for both
 // particles (vpm_set_symmetric_min_n changes it).  Measured crossover of the fused sum:
-// one-sided 650 / 679 / 699 against both-sides 584 / 731 / 746 Gpairs/s at 16384 / 24576 /
-// 32768 particles.
+// one-sided 641 / 720 / 738 against both-sides 624 / 718 / 737 Gpairs/s at 16384 / 24576 /
+// 32768 particles (velocity 1155 / 1258 / 1277 against 1160 / 1350 / 1419, PSE 1231 / 1344 /
+// 1374 against 1380 / 1625 / 1728).
 std::atomic<int64_t> g_sym_min_n{24576};
 
 struct DevInfo {
@@ -405,6 +409,36 @@ int zero_out(double* p, int64_t count, cudaStream_t st) {
 
 // Both-sides sweep of an FP32 self sum (vpm_rot.cuh): launch 0 on the diagonal tiles, then
 // ceil(floor(nt/2) / m) launches of m diagonal pairs each.
+// A second stream per device for the both-sides sweep's diagonal tiles, with the two events
+// that fork it from and join it to the caller's stream.  Created on first use; g_side_mu
+// serialises the fork-launch-join sequence, so calls from several host threads never mix
+// their events.
+struct SideStream {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+std::mutex g_side_mu;
+std::map<int, SideStream> g_side;
+
+// The calling thread holds g_side_mu.
+int side_stream(SideStream** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  auto it = g_side.find(dev);
+  if (it == g_side.end()) {
+    SideStream ss;
+    e = cudaStreamCreateWithFlags(&ss.stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreateWithFlags(side stream)");
+    e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreateWithFlags(side stream)");
+    it = g_side.emplace(dev, ss).first;
+  }
+  *out = &it->second;
+  return VPM_OK;
+}
+
 template <class Op>
 struct RotSweep {
   static constexpr int NV = Op::NV;
@@ -422,8 +456,12 @@ struct RotSweep {
            sets(1) * set_bytes(n) <= max_partial_bytes;
   }
   // accumulator sets of a plan with m diagonal pairs per launch: 2 per pair, and at least the
-  // kRotDiagSplit the diagonal tiles' launch writes
-  static int64_t sets(int m) { return 2 * m > kRotDiagSplit ? 2 * m : kRotDiagSplit; }
+  // kRotDiagSplit the diagonal tiles' launch writes (after the pairs' sets when it runs beside
+  // the pairs' launch)
+  static int64_t sets(int m, bool beside = false) {
+    if (beside) return 2 * m + kRotDiagSplit;
+    return 2 * m > kRotDiagSplit ? 2 * m : kRotDiagSplit;
+  }
 
   // Shared-memory attributes and resident CTAs per SM, once per device (cached like the
   // one-sided sweeps' plans).
@@ -505,9 +543,22 @@ struct RotSweep {
     const int64_t best_w = keep0 ? w0 : w1;
     const double best = double(npairs) * nt / double(slots) / double(best_w);
     if (eff_out) *eff_out = best;
+    // Small n: every pair in one launch that leaves resident-CTA slots free, so the diagonal
+    // tiles' CTAs (a quarter tile of sources each) run beside it in those slots instead of in
+    // a launch of their own before it.
+    const bool beside = best_m >= npairs && best_m * nt < slots &&
+                        sets(best_m, true) * set_bytes(n) <= max_partial_bytes;
+    if (beside) {
+      // create the side stream now, outside any stream capture of the launch that follows
+      std::lock_guard<std::mutex> lk(g_side_mu);
+      SideStream* ss = nullptr;
+      rc = side_stream(&ss);
+      if (rc) return rc;
+    }
+    p->diag_beside = beside ? 1 : 0;
     p->pairs = best_m;
     p->tblocks = nt;
-    p->splits = int(sets(best_m));
+    p->splits = int(sets(best_m, beside));
     p->chunk = n;
     p->smem = kSmem;
     p->threads = kRotThreads;
@@ -516,7 +567,7 @@ struct RotSweep {
     return VPM_OK;
   }
 
-  // acc: [sets(pairs)][NV][n] FP64, zeroed here.
+  // acc: [p.splits][NV][n] FP64, zeroed here.
   static int launch(const Plan& p, const void* rec, int64_t n, double* acc,
                     cudaStream_t st) {
     const int nt = int(tiles(n));
@@ -524,9 +575,37 @@ struct RotSweep {
     int rc = prepare(&occ);
     if (!rc) rc = zero_out(acc, int64_t(p.splits) * NV * n, st);
     if (rc) return rc;
+    cudaError_t e = cudaSuccess;
+    if (p.diag_beside) {
+      // the pairs' launch first on the caller's stream, then the diagonal tiles on the side
+      // stream into sets [2 pairs, 2 pairs + kRotDiagSplit); the caller's stream waits for
+      // both (fork and join by events, so CUDA-graph capture records the same dependencies)
+      std::lock_guard<std::mutex> lk(g_side_mu);
+      SideStream* ss = nullptr;
+      rc = side_stream(&ss);
+      if (rc) return rc;
+      e = cudaEventRecord(ss->fork, st);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord(fork)");
+      rot_sweep_kernel<Op, false><<<(nt / 2) * nt, kRotThreads, kSmem, st>>>(
+          RotArgs{rec, n, nt, 1, acc});
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
+      e = cudaStreamWaitEvent(ss->stream, ss->fork, 0);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent(fork)");
+      RotArgs d{rec, n, nt, 0, acc};
+      d.set0 = 2 * p.pairs;
+      rot_sweep_kernel<Op, true><<<nt * kRotDiagSplit, kRotThreads, kSmem, ss->stream>>>(d);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
+      e = cudaEventRecord(ss->join, ss->stream);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord(join)");
+      e = cudaStreamWaitEvent(st, ss->join, 0);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent(join)");
+      return VPM_OK;
+    }
     rot_sweep_kernel<Op, true><<<nt * kRotDiagSplit, kRotThreads, kSmem, st>>>(
         RotArgs{rec, n, nt, 0, acc});
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
     const int npairs = nt / 2;
     for (int k0 = 1; k0 <= npairs; k0 += p.pairs) {

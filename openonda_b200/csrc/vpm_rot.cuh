@@ -108,6 +108,7 @@ struct RotArgs {
   int nt;       // tiles of the operator's rot_tile particles
   int k0;       // first diagonal of this launch (0 = the diagonal tiles)
   double* acc;  // accumulators [sets][NV][n]
+  int set0 = 0;  // the diagonal tiles' launch: its first accumulator set
 };
 
 // Particles per tile: kP packed FP32x2 target lanes (2 kP targets) per thread.
@@ -708,8 +709,8 @@ rot_sweep_kernel(const RotArgs a) {
   if (DIAG) {
     I = J = blockIdx.x / kRotDiagSplit;
     h = blockIdx.x - I * kRotDiagSplit;
-    set_i = h;  // each part into its own set: one writer per element
-    set_j = h;
+    set_i = a.set0 + h;  // each part into its own set: one writer per element
+    set_j = a.set0 + h;
   } else {
     const int q = blockIdx.x / a.nt, r = blockIdx.x - q * a.nt;
     const int k = a.k0 + q, n1 = a.nt - k;
