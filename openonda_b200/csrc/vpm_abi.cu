@@ -457,9 +457,9 @@ struct RotSweep {
   }
   // accumulator sets of a plan with m diagonal pairs per launch: 2 per pair, and at least the
   // kRotDiagSplit the diagonal tiles' launch writes (after the pairs' sets when it runs beside
-  // the pairs' launch)
+  // the pair launches)
   static int64_t sets(int m, bool beside = false) {
-    if (beside) return 2 * m + kRotDiagSplit;
+    if (beside) return 2 * int64_t(m) + kRotDiagSplit;
     return 2 * m > kRotDiagSplit ? 2 * m : kRotDiagSplit;
   }
 
@@ -514,7 +514,9 @@ struct RotSweep {
     // launches take the fewest waves in all (the smaller m on a tie).  m0 is kept unless m1
     // saves more than 1 % of the waves: at equal wave counts the launches of m0 measured up to
     // 5 % faster (fused sum at 65536, LES sums at 262144), while m1 gains 1.5 % at 2^20 and 7 %
-    // at 49152.
+    // at 49152.  (Splitting each tile pair's sources over several CTAs, to fill the waves at
+    // small n, measured slower: every part repeats the target side's carries and final FP64
+    // atomics, and the sets to zero and sum multiply.)
     int m0 = 1;
     double be = -1.0;
     for (int m = 1; m <= kMaxPairs && m <= npairs; ++m) {
@@ -543,11 +545,13 @@ struct RotSweep {
     const int64_t best_w = keep0 ? w0 : w1;
     const double best = double(npairs) * nt / double(slots) / double(best_w);
     if (eff_out) *eff_out = best;
-    // Small n: every pair in one launch that leaves resident-CTA slots free, so the diagonal
-    // tiles' CTAs (a quarter tile of sources each) run beside it in those slots instead of in
-    // a launch of their own before it.
-    const bool beside = best_m >= npairs && best_m * nt < slots &&
-                        sets(best_m, true) * set_bytes(n) <= max_partial_bytes;
+    // Small n (pair launches of at most 64 waves of whole tile pairs): the diagonal tiles' CTAs
+    // (a quarter tile of sources each) run beside the pair launches on a second stream, into
+    // four sets of their own, and take the slots their waves leave free, instead of a launch
+    // of their own before them.  Measured (Gpairs/s, own launch -> beside): fused sum 574 ->
+    // 622 at 16384, 739 -> 748 at 32768; velocity 1427 -> 1477 and PSE 1733 -> 1808 at 32768;
+    // 1-2 % at 49152.  At large n that launch is a few tenths of a percent of the sweep.
+    const bool beside = best_w <= 64 && sets(best_m, true) * set_bytes(n) <= max_partial_bytes;
     if (beside) {
       // create the side stream now, outside any stream capture of the launch that follows
       std::lock_guard<std::mutex> lk(g_side_mu);
@@ -576,20 +580,32 @@ struct RotSweep {
     if (!rc) rc = zero_out(acc, int64_t(p.splits) * NV * n, st);
     if (rc) return rc;
     cudaError_t e = cudaSuccess;
+    const int npairs = nt / 2;
+    SideStream* ss = nullptr;
+    std::unique_lock<std::mutex> lk(g_side_mu, std::defer_lock);
     if (p.diag_beside) {
-      // the pairs' launch first on the caller's stream, then the diagonal tiles on the side
-      // stream into sets [2 pairs, 2 pairs + kRotDiagSplit); the caller's stream waits for
-      // both (fork and join by events, so CUDA-graph capture records the same dependencies)
-      std::lock_guard<std::mutex> lk(g_side_mu);
-      SideStream* ss = nullptr;
+      // the pair launches on the caller's stream, the diagonal tiles on the side stream into
+      // sets [sets of the pairs, + kRotDiagSplit); the caller's stream waits for both (fork
+      // and join by events, so CUDA-graph capture records the same dependencies)
+      lk.lock();
       rc = side_stream(&ss);
       if (rc) return rc;
       e = cudaEventRecord(ss->fork, st);
       if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord(fork)");
-      rot_sweep_kernel<Op, false><<<(nt / 2) * nt, kRotThreads, kSmem, st>>>(
-          RotArgs{rec, n, nt, 1, acc});
+    } else {
+      rot_sweep_kernel<Op, true><<<nt * kRotDiagSplit, kRotThreads, kSmem, st>>>(
+          RotArgs{rec, n, nt, 0, acc});
       e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
+    }
+    for (int k0 = 1; k0 <= npairs; k0 += p.pairs) {
+      const int m = (npairs - k0 + 1 < p.pairs) ? npairs - k0 + 1 : p.pairs;
+      rot_sweep_kernel<Op, false><<<m * nt, kRotThreads, kSmem, st>>>(
+          RotArgs{rec, n, nt, k0, acc});
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
+    }
+    if (p.diag_beside) {
       e = cudaStreamWaitEvent(ss->stream, ss->fork, 0);
       if (e != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent(fork)");
       RotArgs d{rec, n, nt, 0, acc};
@@ -601,19 +617,6 @@ struct RotSweep {
       if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord(join)");
       e = cudaStreamWaitEvent(st, ss->join, 0);
       if (e != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent(join)");
-      return VPM_OK;
-    }
-    rot_sweep_kernel<Op, true><<<nt * kRotDiagSplit, kRotThreads, kSmem, st>>>(
-        RotArgs{rec, n, nt, 0, acc});
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
-    const int npairs = nt / 2;
-    for (int k0 = 1; k0 <= npairs; k0 += p.pairs) {
-      const int m = (npairs - k0 + 1 < p.pairs) ? npairs - k0 + 1 : p.pairs;
-      rot_sweep_kernel<Op, false><<<m * nt, kRotThreads, kSmem, st>>>(RotArgs{rec, n, nt, k0,
-                                                                              acc});
-      e = cudaGetLastError();
-      if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
     }
     return VPM_OK;
   }
