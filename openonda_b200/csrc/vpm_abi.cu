@@ -90,7 +90,8 @@ struct Plan {
   int r = 0;
   int nv = 0;
   int pairs = 0;  // both-sides sweep (vpm_rot.cuh): diagonal pairs per launch; 0 = one-sided
-  int variant = 0;  // both-sides fused sum: 0 = built for VPM_ROT_MINB CTAs/SM, 1 = _ALT
+  // both-sides fused sum: 0 = built for VPM_ROT_MINB CTAs/SM, 1 = _ALT, 2 = 512-particle tiles
+  int variant = 0;
   // both-sides sweep: the diagonal tiles run beside the (single) diagonal-pair launch on a
   // second stream, into their own accumulator sets after the pairs' ones
   int diag_beside = 0;
@@ -726,6 +727,7 @@ struct Ops {
   using LesStep = OpLesStep<T, REFINE, UC>;
   using VelStretchBoth = OpVelStretchBoth<REFINE, UC>;  // FP32 only
   using VelStretchBothAlt = OpVelStretchBoth<REFINE, UC, VPM_ROT_MINB_ALT>;
+  using VelStretchBothSmall = OpVelStretchBoth<REFINE, UC, VPM_ROT_MINB_ALT, 2>;
   using VelBoth = OpVelBoth<REFINE, UC>;                // FP32 only
   using PseBoth = OpPseBoth<REFINE, UC>;                // FP32 only
   using LesStepBoth = OpLesStepBoth<REFINE, UC>;        // FP32 only
@@ -769,19 +771,34 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
       if constexpr (LaneTraits<T>::kLanes == 2) {
         if (RotSweep<typename O::VelStretchBoth>::usable(m, n, mpb)) {
-          // two builds of the fused sum (3 and 2 resident CTAs per SM, the same tiles): take
-          // the one whose launches fill the waves better, the 2-CTA build on a tie (it
-          // measured equal or faster whenever its waves were as full)
-          Plan pa, pb;
-          double ea = 0.0, eb = 0.0;
+          // two builds of the fused sum on 768-particle tiles (3 and 2 resident CTAs per SM):
+          // take the one whose launches fill the waves better, the 2-CTA build on a tie (it
+          // measured equal or faster whenever its waves were as full).  A third on
+          // 512-particle tiles (4 targets per lane, 2 CTAs per SM) evaluates pairs at about
+          // 0.92 of their rate but makes 2.25x the tile pairs, so it fills the waves where
+          // few 768-particle tiles do not (24576: 728 -> 768, 32768: 748 -> 790 Gpairs/s;
+          // 49152 and up 6-9 % slower): taken when 0.92 of its fill beats theirs by 1 %.
+          constexpr double kSmallTileRate = 0.92;
+          Plan pa, pb, pc;
+          double ea = 0.0, eb = 0.0, ec = 0.0;
           int rc = RotSweep<typename O::VelStretchBoth>::plan(n, &pa, mpb, &ea);
           if (!rc) rc = RotSweep<typename O::VelStretchBothAlt>::plan(n, &pb, mpb, &eb);
           if (rc) return rc;
+          double e = ea;
           if (eb >= ea - 0.01) {
             pb.variant = 1;
             *p = pb;
+            e = eb;
           } else {
             *p = pa;
+          }
+          if (RotSweep<typename O::VelStretchBothSmall>::usable(m, n, mpb)) {
+            rc = RotSweep<typename O::VelStretchBothSmall>::plan(n, &pc, mpb, &ec);
+            if (rc) return rc;
+            if (kSmallTileRate * ec > e + 0.01) {
+              pc.variant = 2;
+              *p = pc;
+            }
           }
           return VPM_OK;
         }
@@ -952,7 +969,9 @@ int run(const Call& c) {
       return rc;
     case VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS:
       if constexpr (LaneTraits<T>::kLanes == 2) {
-        if (p.pairs && p.variant)  // m == n: the targets are all the records (tgt_begin == 0)
+        if (p.pairs && p.variant == 2)  // m == n: the targets are all the records
+          rc = RotSweep<typename O::VelStretchBothSmall>::launch(p, src, c.n, part, c.st);
+        else if (p.pairs && p.variant == 1)
           rc = RotSweep<typename O::VelStretchBothAlt>::launch(p, src, c.n, part, c.st);
         else if (p.pairs)
           rc = RotSweep<typename O::VelStretchBoth>::launch(p, src, c.n, part, c.st);

@@ -229,11 +229,11 @@ struct RotStd {
 
 // Fused velocity + stretching, both sides of the pair (FP32x2 lanes).  Built for 3 and for 2
 // resident CTAs per SM (MINB); the planner takes the one whose launches fill the waves better.
-template <bool REFINE, bool UC, int MINB = VPM_ROT_MINB>
+template <bool REFINE, bool UC, int MINB = VPM_ROT_MINB, int P = VPM_ROT_P>
 struct OpVelStretchBoth : RotStd<OpVelStretch<float2, REFINE, UC>, UC> {
   using V = float2;
   static constexpr int NV = 9;
-  static constexpr int kP = VPM_ROT_P;
+  static constexpr int kP = P;
   static constexpr int kMinBlocks = MINB;
   static constexpr int kUnroll = VPM_ROT_UNROLL;
   static constexpr int kSrcWindow = VPM_ROT_SRC_WINDOW;

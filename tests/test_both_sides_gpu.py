@@ -97,6 +97,32 @@ def test_both_sides_vs_fp64(n, ring, uniform_core):
     assert kernels.device_errors() == 0
 
 
+@pytest.mark.parametrize("uniform_core", [False, True])
+def test_small_tile_build_vs_fp64(uniform_core):
+    """N = 32768: the planner takes the fused sum's 512-particle-tile build (4 targets per
+    thread), whose 2016 tile pairs fill the waves where 903 of 768 particles do not."""
+    from openonda_b200 import kernels
+
+    n = 32768
+    p = kernels.plan_info("velocity_and_strength_gradients", "fp32c", n, n, uniform_core)
+    assert p["targets_per_thread"] == 4, p
+    f = _field(n, 11, False)
+    if uniform_core:
+        f.radii[:] = f.radii[0]
+    x, a, s = _dev32(f)
+    ref = kernels.velocity_and_strength_gradients(x, a, s, precision="fp64")
+    both = kernels.velocity_and_strength_gradients(x, a, s, precision="fp32c",
+                                                   uniform_core=uniform_core)
+    again = kernels.velocity_and_strength_gradients(x, a, s, precision="fp32c",
+                                                    uniform_core=uniform_core)
+    for k in range(2):
+        e = normwise(both[k].cpu().numpy(), ref[k].cpu().numpy())
+        print(f"n={n} uc={uniform_core} k={k}: {e:.2e}")
+        assert e <= (1e-6 if k == 0 else 2e-6), (k, e)
+        assert torch.equal(both[k], again[k])  # deterministic
+    assert kernels.device_errors() == 0
+
+
 def test_both_sides_is_deterministic(both_sides_always):
     from openonda_b200 import kernels
 
