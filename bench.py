@@ -527,7 +527,9 @@ def main():
             "dtype": "f32 pair terms + f64 carries", "data": "synthetic",
             "config": {"workload": workload_name(n, args.seed), "n": n,
                        "precision": args.precision,
-                       "parallelism": f"target shards x{world}, sources all-gathered",
+                       "parallelism": (f"pair shards x{world}, records all-gathered, "
+                                       "FP64 rows reduce-scattered" if sweep32.pairs is not None
+                                       else f"target shards x{world}, sources all-gathered"),
                        "l2": "flushed between timed steps (512 MiB write)"},
             "fp64": {"fused_gpairs_s": round(fp64_fused, 3),
                      "dropin_two_sweeps_gpairs_s":

@@ -213,6 +213,31 @@ int vpm_sweep_records(int op, const void* records, int64_t n, int64_t target_beg
                       int ref_extra_4pi, double* out, double* out2, int precision,
                       void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- pair shards across GPUs (VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS, FP32C[_REFINED]) ----
+ * The both-sides schedule of a self sum over n records split between ranks by tiles: rank r
+ * runs the diagonal tiles [tile_begin, tile_end) and the diagonal pairs [pair_begin,
+ * pair_end) of the plan every rank makes for n, over all n gathered records, and sums its
+ * accumulator sets into `rows` (n, values) FP64 -- one particle's sums per row, in a fixed
+ * order.  The sum of all ranks' rows (a reduce-scatter between the GPUs, by row ranges) is
+ * what the single-GPU sweep sums; vpm_finalize_pairs_partial turns a rank's summed rows into
+ * its velocities and stretching.  Replaces, per rank, the target-shard sweep
+ * vpm_sweep_records, which cannot evaluate a pair once for both particles when the two
+ * particles sit on different ranks. */
+/* Tiles, diagonal pairs and diagonal pairs per launch of the plan for n, values per row,
+ * workspace bytes of one vpm_sweep_pairs_partial call (VPM_ERR_ARG if n does not take the
+ * both-sides schedule).  Any output pointer may be NULL. */
+int vpm_pairs_layout(int op, int precision, int64_t n, int64_t* tiles, int64_t* pairs,
+                     int* pairs_per_launch, int* values, size_t* workspace_bytes);
+int vpm_sweep_pairs_partial(int op, const void* records, int64_t n, int64_t tile_begin,
+                            int64_t tile_end, int64_t pair_begin, int64_t pair_end,
+                            double* rows, int precision, void* workspace,
+                            size_t workspace_bytes, void* stream);
+/* Outputs of targets records[target_begin, target_begin + m) from their summed rows (m,
+ * values): out = velocities (m,3), out2 = stretching (m,3). */
+int vpm_finalize_pairs_partial(int op, const double* rows, const void* records,
+                               int64_t target_begin, int64_t m, double* out, double* out2,
+                               int precision, void* stream);
+
 /* ---- device-resident time step (vpmModule.ParticleSystem), element-wise, HBM-bound ------ */
 /* out = x + c k over `count` doubles: RK stages (vpmModule.py:580,604,637,641,676,680,684). */
 int vpm_axpy(const double* x, const double* k, double c, int64_t count, double* out,

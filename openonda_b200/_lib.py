@@ -72,6 +72,10 @@ SIGNATURES = {
     "vpm_record_bytes": ([_I], _SZ),
     "vpm_pack_records": ([_P, _P, _P, _P, _I64, _I, _P, _P], _I),
     "vpm_sweep_records": ([_I, _P, _I64, _I64, _I64, _I, _P, _P, _I, _P, _SZ, _P], _I),
+    "vpm_pairs_layout": ([_I, _I, _I64, _P, _P, _P, _P, _P], _I),
+    "vpm_sweep_pairs_partial": ([_I, _P, _I64, _I64, _I64, _I64, _I64, _P, _I, _P, _SZ, _P],
+                                _I),
+    "vpm_finalize_pairs_partial": ([_I, _P, _P, _I64, _I64, _P, _P, _I, _P], _I),
     "vpm_selfinduced_velocity_noalloc": ([_P, _P, _P, _I64, _P, _I, _P], _I),
     "vpm_axpy": ([_P, _P, ctypes.c_double, _I64, _P, _P], _I),
     "vpm_rk4_combine": ([_P, _P, _P, _P, _P, ctypes.c_double, _I64, _P, _P], _I),

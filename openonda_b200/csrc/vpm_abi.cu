@@ -286,14 +286,12 @@ __device__ __forceinline__ void sum_splits(const double* __restrict__ part, int 
   }
 }
 
+// The outputs of target i from its summed values v (KIND: which sums, which scaling).
 template <class T, int KIND, int NV>
-__global__ void finalize_vec_kernel(const double* __restrict__ part, int splits, int64_t m,
-                                    const Rec<T>* __restrict__ tgt, double* __restrict__ out,
-                                    double* __restrict__ out2, double* __restrict__ out3) {
-  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= m) return;
-  double v[NV];
-  sum_splits<NV>(part, splits, m, i, v);
+__device__ __forceinline__ void finalize_values(const double (&v)[NV], const Rec<T>* tgt,
+                                                int64_t i, double* __restrict__ out,
+                                                double* __restrict__ out2,
+                                                double* __restrict__ out3) {
   if constexpr (KIND == FIN_VEL) {
     out[3 * i] = -v[0] * kOneOver4Pi;
     out[3 * i + 1] = -v[1] * kOneOver4Pi;
@@ -329,6 +327,44 @@ __global__ void finalize_vec_kernel(const double* __restrict__ part, int splits,
     so[3 * i + 1] = (bz * Ax - bx * Az + 3.0 * v[o + 4]) * kOneOver4Pi;
     so[3 * i + 2] = (bx * Ay - by * Ax + 3.0 * v[o + 5]) * kOneOver4Pi;
   }
+}
+
+template <class T, int KIND, int NV>
+__global__ void finalize_vec_kernel(const double* __restrict__ part, int splits, int64_t m,
+                                    const Rec<T>* __restrict__ tgt, double* __restrict__ out,
+                                    double* __restrict__ out2, double* __restrict__ out3) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double v[NV];
+  sum_splits<NV>(part, splits, m, i, v);
+  finalize_values<T, KIND, NV>(v, tgt, i, out, out2, out3);
+}
+
+// Pair shards across GPUs: rows[i][v] = the sum over the sets s, in order, of acc[s][v][i].
+// One particle's NV sums in a row, so each rank's target rows are one contiguous block for
+// the reduce-scatter between the GPUs.
+template <int NV>
+__global__ void sets_to_rows_kernel(const double* __restrict__ acc, int sets, int64_t n,
+                                    double* __restrict__ rows) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v[NV];
+  sum_splits<NV>(acc, sets, n, i, v);
+#pragma unroll
+  for (int k = 0; k < NV; ++k) rows[i * NV + k] = v[k];
+}
+
+// The outputs of targets [0, m) (records tgt) from their summed rows (m, NV).
+template <class T, int KIND, int NV>
+__global__ void finalize_rows_kernel(const double* __restrict__ rows, int64_t m,
+                                     const Rec<T>* __restrict__ tgt, double* __restrict__ out,
+                                     double* __restrict__ out2) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double v[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = rows[i * NV + k];
+  finalize_values<T, KIND, NV>(v, tgt, i, out, out2, nullptr);
 }
 
 constexpr int kReduceThreads = 1024;
@@ -618,6 +654,36 @@ struct RotSweep {
       if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord(join)");
       e = cudaStreamWaitEvent(st, ss->join, 0);
       if (e != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent(join)");
+    }
+    return VPM_OK;
+  }
+
+  // Part of a sweep (pair shards across GPUs): the diagonal tiles [t_begin, t_end) and the
+  // diagonal pairs k in [k_begin, k_end) (k = 1 .. nt / 2), in launches of p.pairs pairs, on
+  // the caller's stream into the sets of a plan without the side stream.
+  // acc: [sets(p.pairs)][NV][n] FP64, zeroed here.
+  static int launch_part(const Plan& p, const void* rec, int64_t n, double* acc, int t_begin,
+                         int t_end, int k_begin, int k_end, cudaStream_t st) {
+    const int nt = int(tiles(n));
+    int occ = 1;
+    int rc = prepare(&occ);
+    if (!rc) rc = zero_out(acc, sets(p.pairs) * NV * n, st);
+    if (rc) return rc;
+    cudaError_t e = cudaSuccess;
+    if (t_end > t_begin) {
+      RotArgs d{rec, n, nt, 0, acc};
+      d.tile0 = t_begin;
+      rot_sweep_kernel<Op, true><<<(t_end - t_begin) * kRotDiagSplit, kRotThreads, kSmem, st>>>(
+          d);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
+    }
+    for (int k0 = k_begin; k0 < k_end; k0 += p.pairs) {
+      const int m = (k_end - k0 < p.pairs) ? k_end - k0 : p.pairs;
+      rot_sweep_kernel<Op, false><<<m * nt, kRotThreads, kSmem, st>>>(
+          RotArgs{rec, n, nt, k0, acc});
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
     }
     return VPM_OK;
   }
@@ -1417,6 +1483,28 @@ int noalloc_scratch(void** out) {
 
 using namespace vpm;
 
+// ---- pair shards across GPUs: the fused sum's both-sides schedule split by tile ranges ----
+// Calls f(RotSweep<X>{}, plan) for the both-sides build the planner takes for a self sum of n
+// particles (every rank plans the same n, so all ranks use the same tiles and launch sizes).
+template <class T, bool REFINE, bool UC, class F>
+int with_fused_both(int64_t n, F&& f) {
+  using O = Ops<T, REFINE, UC>;
+  if constexpr (LaneTraits<T>::kLanes != 2) {
+    return fail(VPM_ERR_ARG, "pair shards need an FP32-compensated precision");
+  } else {
+    Plan p;
+    int rc = plan_op<T, REFINE, UC>(VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS, n, n, &p);
+    if (rc) return rc;
+    if (!p.pairs)
+      return fail(VPM_ERR_ARG, "n = " + std::to_string(n) +
+                                   " does not take the both-sides schedule "
+                                   "(vpm_set_symmetric_min_n); shard the targets instead");
+    if (p.variant == 2) return f(RotSweep<typename O::VelStretchBothSmall>{}, p);
+    if (p.variant == 1) return f(RotSweep<typename O::VelStretchBothAlt>{}, p);
+    return f(RotSweep<typename O::VelStretchBoth>{}, p);
+  }
+}
+
 extern "C" {
 
 int vpm_abi_version(void) { return VPM_ABI_VERSION; }
@@ -1461,6 +1549,92 @@ size_t vpm_workspace_bytes(int op, int precision, int64_t m, int64_t n) {
     return r;
   });
   return rc ? 0 : total;
+}
+
+int vpm_pairs_layout(int op, int precision, int64_t n, int64_t* tiles, int64_t* pairs,
+                     int* pairs_per_launch, int* values, size_t* workspace_bytes) {
+  if (op != VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS)
+    return fail(VPM_ERR_ARG, "pair shards are built for the fused velocity + stretching sum");
+  if (n < 0) return fail(VPM_ERR_ARG, "negative size");
+  return with_precision(precision, [&](auto P) {
+    using Pp = decltype(P);
+    return with_fused_both<typename Pp::type, Pp::refine, Pp::uc>(n, [&](auto rs,
+                                                                        const Plan& p) {
+      using RS = decltype(rs);
+      const int64_t nt = RS::tiles(n);
+      if (tiles) *tiles = nt;
+      if (pairs) *pairs = nt / 2;
+      if (pairs_per_launch) *pairs_per_launch = p.pairs;
+      if (values) *values = RS::NV;
+      if (workspace_bytes) *workspace_bytes = size_t(RS::sets(p.pairs)) * RS::set_bytes(n);
+      return VPM_OK;
+    });
+  });
+}
+
+int vpm_sweep_pairs_partial(int op, const void* records, int64_t n, int64_t tile_begin,
+                            int64_t tile_end, int64_t pair_begin, int64_t pair_end,
+                            double* rows, int precision, void* workspace,
+                            size_t workspace_bytes, void* stream) {
+  if (op != VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS)
+    return fail(VPM_ERR_ARG, "pair shards are built for the fused velocity + stretching sum");
+  if (n <= 0) return fail(VPM_ERR_ARG, "n must be positive");
+  if (!records || !rows || !workspace) return fail(VPM_ERR_ARG, "null pointer");
+  if (reinterpret_cast<uintptr_t>(records) % 16 != 0)
+    return fail(VPM_ERR_ALIGN, "records must be 16-byte aligned");
+  if (reinterpret_cast<uintptr_t>(workspace) % kAlign != 0)
+    return fail(VPM_ERR_ALIGN, "workspace must be 256-byte aligned");
+  int rc = check_arch();
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return with_precision(precision, [&](auto P) {
+    using Pp = decltype(P);
+    return with_fused_both<typename Pp::type, Pp::refine, Pp::uc>(n, [&](auto rs,
+                                                                        const Plan& p) {
+      using RS = decltype(rs);
+      const int64_t nt = RS::tiles(n);
+      if (tile_begin < 0 || tile_end < tile_begin || tile_end > nt)
+        return fail(VPM_ERR_ARG, "tile range outside [0, " + std::to_string(nt) + ")");
+      if (pair_begin < 0 || pair_end < pair_begin || pair_end > nt / 2)
+        return fail(VPM_ERR_ARG, "pair range outside [0, " + std::to_string(nt / 2) + ")");
+      const size_t need = size_t(RS::sets(p.pairs)) * RS::set_bytes(n);
+      if (workspace_bytes < need)
+        return fail(VPM_ERR_WORKSPACE, "workspace has " + std::to_string(workspace_bytes) +
+                                           " bytes, needs " + std::to_string(need));
+      double* acc = static_cast<double*>(workspace);
+      int r = RS::launch_part(p, records, n, acc, int(tile_begin), int(tile_end),
+                              int(pair_begin) + 1, int(pair_end) + 1, st);
+      if (r) return r;
+      sets_to_rows_kernel<RS::NV><<<unsigned((n + 255) / 256), 256, 0, st>>>(
+          acc, int(RS::sets(p.pairs)), n, rows);
+      cudaError_t e = cudaGetLastError();
+      return e == cudaSuccess ? VPM_OK : cuda_fail(e, "rows launch");
+    });
+  });
+}
+
+int vpm_finalize_pairs_partial(int op, const double* rows, const void* records,
+                               int64_t target_begin, int64_t m, double* out, double* out2,
+                               int precision, void* stream) {
+  if (op != VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS)
+    return fail(VPM_ERR_ARG, "pair shards are built for the fused velocity + stretching sum");
+  if (m < 0 || target_begin < 0) return fail(VPM_ERR_ARG, "negative size or offset");
+  if (m == 0) return VPM_OK;
+  if (!rows || !records || !out || !out2) return fail(VPM_ERR_ARG, "null pointer");
+  if (reinterpret_cast<uintptr_t>(records) % 16 != 0)
+    return fail(VPM_ERR_ALIGN, "records must be 16-byte aligned");
+  const int pr = precision & ~VPM_UNIFORM_CORE;
+  if (pr != VPM_FP32C && pr != VPM_FP32C_REFINED)
+    return fail(VPM_ERR_ARG, "pair shards need an FP32-compensated precision");
+  int rc = check_arch();
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const Rec<float2>* tgt = static_cast<const Rec<float2>*>(records) + target_begin;
+  static_assert(OpVelStretchBoth<false, false>::NV == 9, "the fused sum's 9 values per row");
+  finalize_rows_kernel<float2, FIN_VELSTRETCH, 9><<<unsigned((m + 255) / 256), 256, 0, st>>>(
+      rows, m, tgt, out, out2);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? VPM_OK : cuda_fail(e, "finalize launch");
 }
 
 int vpm_plan_info(int op, int precision, int64_t m, int64_t n, int64_t* target_blocks,

@@ -108,7 +108,8 @@ struct RotArgs {
   int nt;       // tiles of the operator's rot_tile particles
   int k0;       // first diagonal of this launch (0 = the diagonal tiles)
   double* acc;  // accumulators [sets][NV][n]
-  int set0 = 0;  // the diagonal tiles' launch: its first accumulator set
+  int set0 = 0;   // the diagonal tiles' launch: its first accumulator set
+  int tile0 = 0;  // the diagonal tiles' launch: its first tile (a part of a sweep)
 };
 
 // Particles per tile: kP packed FP32x2 target lanes (2 kP targets) per thread.
@@ -707,8 +708,9 @@ rot_sweep_kernel(const RotArgs a) {
   int I, J, set_i, set_j;
   int h = 0;  // DIAG: which part of the tile's sources this CTA takes
   if (DIAG) {
-    I = J = blockIdx.x / kRotDiagSplit;
-    h = blockIdx.x - I * kRotDiagSplit;
+    const int t = blockIdx.x / kRotDiagSplit;
+    h = blockIdx.x - t * kRotDiagSplit;
+    I = J = a.tile0 + t;
     set_i = a.set0 + h;  // each part into its own set: one writer per element
     set_j = a.set0 + h;
   } else {

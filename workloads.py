@@ -378,6 +378,75 @@ def sweeps(args):
                    "gpairs_per_s": round(float(n) * n / (ms / 1e3) / 1e9, 1)})
 
 
+def pairshards(args):
+    """Each rank's share of a multi-GPU sweep of the fused sum, timed on this one GPU (the
+    ranks run in turn; the collectives are not part of it): pair shards (the both-sides
+    schedule split by tiles and diagonal pairs, vpm_sweep_pairs_partial + the FP64 rows)
+    against target shards (vpm_sweep_records, one-sided, N / world targets).  The slowest
+    rank sets the step, so the projected rate is N^2 over the slowest rank's time; the
+    exchanges it leaves out move 64 MB (records) and, for pair shards, 72 MB (rows) at
+    N = 2^20."""
+    from openonda_b200 import _lib
+    from openonda_b200.distributed import (pair_shard_ranges, pairs_layout, shard_range,
+                                           sweep_pairs_partial)
+
+    n = args.n or (1 << 20)
+    f = configs.random_cloud(n, seed=0)
+    r32 = lambda z: torch.from_numpy(np.asarray(z, np.float32).astype(np.float64)).cuda()
+    x, a, s = r32(f.positions), r32(f.strengths), r32(f.radii)
+    lib = _lib.load()
+    code = _lib.precision_code("fp32c")
+    rec = torch.empty((n, int(lib.vpm_record_bytes(code)) // 4), dtype=torch.float32,
+                      device=x.device)
+    _lib.check(lib.vpm_pack_records(x.data_ptr(), a.data_ptr(), s.data_ptr(), None, n, code,
+                                    rec.data_ptr(), torch.cuda.current_stream().cuda_stream))
+    nt, npairs, per, nv, wsb = pairs_layout(n, "fp32c")
+    ws = torch.empty(max(wsb, 256), dtype=torch.uint8, device=x.device)
+    rows = torch.empty((n, nv), dtype=torch.float64, device=x.device)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=x.device)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    t1 = timed(lambda: kernels.velocity_and_strength_gradients(x, a, s, precision="fp32c"))
+    _emit({"workload": "pairshards", "n": n, "world": 1, "ms": round(t1, 2),
+           "gpairs_per_s": round(float(n) * n / t1 / 1e6, 1)})
+    for world in args.sizes or (2, 4, 8):
+        pair_ms, tgt_ms = [], []
+        for r in range(world):
+            t0_, t1_, p0, p1 = pair_shard_ranges(nt, npairs, r, world)
+            pair_ms.append(timed(lambda: sweep_pairs_partial(rec, n, (t0_, t1_), (p0, p1),
+                                                             rows, ws, "fp32c")))
+            lo, hi = shard_range(n, r, world)
+            m = hi - lo
+            nb = kernels.workspace_bytes("velocity_and_strength_gradients", "fp32c", m, n)
+            wst = torch.empty(max(nb, 256), dtype=torch.uint8, device=x.device)
+            u = torch.empty((m, 3), dtype=torch.float64, device=x.device)
+            g = torch.empty_like(u)
+            tgt_ms.append(timed(lambda: _lib.check(lib.vpm_sweep_records(
+                _lib.OPS["velocity_and_strength_gradients"], rec.data_ptr(), n, lo, m, 0,
+                u.data_ptr(), g.data_ptr(), code, wst.data_ptr(), wst.numel(),
+                torch.cuda.current_stream().cuda_stream))))
+            del wst
+        tp, tt = max(pair_ms), max(tgt_ms)
+        _emit({"workload": "pairshards", "n": n, "world": world,
+               "pair_shards": {"slowest_rank_ms": round(tp, 2),
+                               "fastest_rank_ms": round(min(pair_ms), 2),
+                               "projected_gpairs_per_s": round(float(n) * n / tp / 1e6, 1),
+                               "per_gpu_vs_one_gpu": round(t1 / (world * tp), 3)},
+               "target_shards": {"slowest_rank_ms": round(tt, 2),
+                                 "projected_gpairs_per_s": round(float(n) * n / tt / 1e6, 1),
+                                 "per_gpu_vs_one_gpu": round(t1 / (world * tt), 3)}})
+
+
 def peaks(args):
     """Throughput of the FP32 pipes by microbenchmark (vpm_launch_fma_peak), at three
     occupancies: scalar FFMA, packed FFMA2, a 1:1 mix of the two, and MUFU rsqrt; in lane
@@ -549,7 +618,8 @@ def reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("workload", choices=["config1", "config2", "config3", "config4", "config5",
-                                         "stepkernels", "sweeps", "peaks", "reference"])
+                                         "stepkernels", "sweeps", "peaks", "reference",
+                                         "pairshards"])
     ap.add_argument("--cpu-seconds", type=float, default=None)
     ap.add_argument("--les-coefficient", default="reference",
                     choices=["reference", "least_squares"])
