@@ -446,23 +446,30 @@ int zero_out(double* p, int64_t count, cudaStream_t st) {
 
 // Both-sides sweep of an FP32 self sum (vpm_rot.cuh): launch 0 on the diagonal tiles, then
 // ceil(floor(nt/2) / m) launches of m diagonal pairs each.
-// A second stream per device for the both-sides sweep's diagonal tiles, with the two events
-// that fork it from and join it to the caller's stream.  Created on first use; g_side_mu
-// serialises the fork-launch-join sequence, so calls from several host threads never mix
-// their events.
+int current_context(void** ctx);
+
+// A second stream per device and context for the both-sides sweep's diagonal tiles, with the
+// two events that fork it from and join it to the caller's stream.  Created on first use
+// with that context current (a stream belongs to one context, so another context, or the
+// same device after a reset, gets its own); g_side_mu serialises the fork-launch-join
+// sequence, so calls from several host threads never mix their events.
 struct SideStream {
   cudaStream_t stream = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
 };
 std::mutex g_side_mu;
-std::map<int, SideStream> g_side;
+std::map<std::pair<int, void*>, SideStream> g_side;
 
 // The calling thread holds g_side_mu.
 int side_stream(SideStream** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-  auto it = g_side.find(dev);
+  void* ctx = nullptr;
+  int rc = current_context(&ctx);
+  if (rc) return rc;
+  const auto key = std::make_pair(dev, ctx);
+  auto it = g_side.find(key);
   if (it == g_side.end()) {
     SideStream ss;
     e = cudaStreamCreateWithFlags(&ss.stream, cudaStreamNonBlocking);
@@ -470,7 +477,7 @@ int side_stream(SideStream** out) {
     e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming);
     if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreateWithFlags(side stream)");
-    it = g_side.emplace(dev, ss).first;
+    it = g_side.emplace(key, ss).first;
   }
   *out = &it->second;
   return VPM_OK;
