@@ -12,9 +12,13 @@ That install needs an OpenFOAM environment (the package's setup.py compiles the 
 extension and raises without FOAM_SRC), so where it fails, the recipe places the two
 pure-Python modules of the VPM pair-sum path -- ``OpenONDA/solvers/VPM/ParticlesPhysicsCuda.py``
 (Numba-CUDA) and ``OpenONDA/solvers/VPM/ParticlesPhysics.py`` (Numba CPU) -- unmodified under
-``baseline/_ref/OpenONDA_VPM/``, which is all that path imports.  The outcome is written to
-``baseline/_ref/INSTALL.json``.  Measurement code loads the modules by file path from there
-(see ``load_reference_module``) and reports them unavailable when the folder is absent.
+``baseline/_ref/OpenONDA_VPM/``, which is all that path imports.  The CPU module's Numba
+``np.dot`` on arrays needs SciPy's BLAS bindings, so SciPy (its wheel from the same offline
+wheelhouse, no dependencies) goes to ``baseline/_ref/deps``, for hosts whose Python lacks it;
+``load_reference_module`` appends that folder to ``sys.path``, after any installed SciPy.
+The outcome is written to ``baseline/_ref/INSTALL.json``.  Measurement code loads the modules
+by file path from there (see ``load_reference_module``) and reports them unavailable when the
+folder is absent.
 """
 from __future__ import annotations
 
@@ -29,6 +33,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 VPM_DIR = os.path.join(REF_DIR, "OpenONDA_VPM")
+DEPS_DIR = os.path.join(REF_DIR, "deps")
 MODULES = ("ParticlesPhysicsCuda.py", "ParticlesPhysics.py")
 
 
@@ -36,6 +41,8 @@ def load_reference_module(name: str):
     """Import ``ParticlesPhysicsCuda`` or ``ParticlesPhysics`` from ``baseline/_ref`` by file
     path; raises FileNotFoundError when the reference is not installed."""
     path = os.path.join(VPM_DIR, name + ".py")
+    if os.path.isdir(DEPS_DIR) and DEPS_DIR not in sys.path:
+        sys.path.append(DEPS_DIR)
     if not os.path.exists(path):
         raise FileNotFoundError(f"{path} is not installed (python baseline/install_ref.py)")
     spec = importlib.util.spec_from_file_location(f"openonda_ref_{name}", path)
@@ -66,6 +73,11 @@ def main() -> int:
                             os.path.join(VPM_DIR, name))
         record["how"] = "VPM physics modules placed unmodified (package install failed)"
         record["modules"] = [os.path.join("OpenONDA", "solvers", "VPM", m) for m in MODULES]
+    dep = [sys.executable, "-m", "pip", "install", "--no-index", "--no-deps", "--find-links",
+           "/opt/wheelhouse", "--target", DEPS_DIR, "scipy"]
+    res = subprocess.run(dep, capture_output=True, text=True)
+    record["deps"] = {"scipy": "installed" if res.returncode == 0 else
+                      (res.stdout + res.stderr).strip().splitlines()[-1:]}
     with open(os.path.join(REF_DIR, "INSTALL.json"), "w") as fh:
         json.dump(record, fh, indent=1)
     print(json.dumps(record))

@@ -292,6 +292,52 @@ def reference_gpu(torch, kernels, dev, x_h, a_h, s_h, n):
                        "(ParticlesPhysicsCuda.py:133-191, :375-445), Numba-CUDA, FP64"}
 
 
+def reference_cpu(x_h, a_h, s_h, n, seconds=4.0):
+    """The reference's own CPU module (ParticlesPhysics.py, Numba njit with prange, unmodified,
+    from baseline/_ref) on all host threads, FP64: velocity through get_induced_velocity_at on
+    a bounded number of target rows against all n sources (exact per-pair work), and the
+    stretching sweep, which has no target-subset entry point, on the first 16384 particles.
+    The fused-equivalent rate (one velocity and one stretching evaluation per pair, as the
+    headline counts one fused evaluation) is 1 / (1 / velocity rate + 1 / stretching rate).
+    Returns {"unavailable": why} when the reference or Numba is missing."""
+    try:
+        sys.path.insert(0, os.path.join(HERE, "baseline"))
+        from install_ref import load_reference_module
+
+        import numba
+
+        mod = load_reference_module("ParticlesPhysics")
+        x, a, s = (np.ascontiguousarray(z[:n]) for z in (x_h, a_h, s_h))
+        t0 = time.perf_counter()
+        mod.get_induced_velocity_at(x[:64], x[:64], a[:64], s[:64])  # JIT
+        mod.get_strength_gradients(x[:64], a[:64], s[:64])
+        jit_s = time.perf_counter() - t0
+        m = 64
+        t0 = time.perf_counter()
+        mod.get_induced_velocity_at(x[:m], x, a, s)
+        rate = m * n / (time.perf_counter() - t0)
+        m = int(min(n, max(64, rate * seconds / n)))
+        t0 = time.perf_counter()
+        mod.get_induced_velocity_at(x[:m], x, a, s)
+        t_vel = time.perf_counter() - t0
+        ns = min(n, 16384)
+        t0 = time.perf_counter()
+        mod.get_strength_gradients(x[:ns], a[:ns], s[:ns])
+        t_str = time.perf_counter() - t0
+    except Exception as e:  # noqa: BLE001 -- the bench reports why and goes on
+        msg = str(e).splitlines()[0] if str(e) else ""
+        return {"unavailable": f"{type(e).__name__}: {msg}"}
+    r_vel = m * float(n) / t_vel / 1e9
+    r_str = float(ns) * ns / t_str / 1e9
+    return {"module": "ParticlesPhysics.py (Numba CPU, FP64)", "numba": numba.__version__,
+            "threads": numba.get_num_threads(), "jit_s": round(jit_s, 1),
+            "velocity_gpairs_s": round(r_vel, 4),
+            "velocity_sample": f"{m} targets x {n} sources, {t_vel:.1f} s",
+            "stretching_gpairs_s": round(r_str, 4),
+            "stretching_sample": f"{ns} x {ns}, {t_str:.1f} s",
+            "fused_equivalent_gpairs_s": round(1.0 / (1.0 / r_vel + 1.0 / r_str), 4)}
+
+
 def load_traffic():
     path = os.path.join(HERE, "profiles", "ncu_traffic.json")
     try:
@@ -426,6 +472,9 @@ def main():
     ref_gpu = None
     if world == 1:
         ref_gpu = reference_gpu(torch, kernels, dev, x_h, a_h, s_h, min(n, 131072))
+    ref_cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        ref_cpu = reference_cpu(x_h, a_h, s_h, n)
     # ---- adjoint: one VJP sweep of the right-hand side (u, S [+ P]) against one forward
     # evaluation of it, N = 65536 random cloud, cotangents N(0,1) ----
     adjoint = None
@@ -539,6 +588,10 @@ def main():
                          None if fp64_dropin is None else round(value / fp64_dropin, 3)},
             "rel_err_vs_fp64": {"velocity": err_u, "stretching": err_g},
             "reference_gpu": ref_gpu,
+            "reference_cpu": ref_cpu,
+            "speedup_vs_reference_cpu":
+                None if not ref_cpu or "fused_equivalent_gpairs_s" not in ref_cpu
+                else round(e2e_value / ref_cpu["fused_equivalent_gpairs_s"], 1),
             "speedup_vs_reference_gpu":
                 None if not ref_gpu or "kernel_gpairs_s" not in ref_gpu
                 else {"kernel": round(value / ref_gpu["kernel_gpairs_s"], 1),
