@@ -453,7 +453,7 @@ def main():
     fp64_fused = float(n) * n / (t64 / args.fp64_steps) / 1e9
     err_u = max_over_ranks(normwise(u32, u64))
     err_g = max_over_ranks(normwise(g32, g64))
-    fp64_dropin = None
+    fp64_dropin = fp64_one_sided = None
     if world == 1:
         xa = torch.from_numpy(x_h).to(dev)
         aa = torch.from_numpy(a_h).to(dev)
@@ -465,6 +465,15 @@ def main():
 
         tdi, _, _ = timed(dropin, 1, 1)
         fp64_dropin = float(n) * n / tdi / 1e9
+        # the plain FP64 kernel: the fused sum one-sided (each ordered pair evaluated for its
+        # target only), as the reference's kernels evaluate it
+        prev = kernels.set_symmetric_min_n(1 << 40)
+        try:
+            tos, _, _ = timed(lambda: kernels.velocity_and_strength_gradients(
+                xa, aa, sa, precision="fp64"), 1, 1)
+        finally:
+            kernels.set_symmetric_min_n(prev)
+        fp64_one_sided = float(n) * n / tos / 1e9
         del xa, aa, sa
 
     # ---- the reference's own Numba-CUDA kernels (ParticlesPhysicsCuda.py, unmodified, from
@@ -581,6 +590,11 @@ def main():
                                        else f"target shards x{world}, sources all-gathered"),
                        "l2": "flushed between timed steps (512 MiB write)"},
             "fp64": {"fused_gpairs_s": round(fp64_fused, 3),
+                     "fused_path": "both-sides" if sweep64.both_sides else "one-sided",
+                     "one_sided_gpairs_s":
+                         None if fp64_one_sided is None else round(fp64_one_sided, 3),
+                     "speedup_vs_fp64_one_sided":
+                         None if fp64_one_sided is None else round(value / fp64_one_sided, 3),
                      "dropin_two_sweeps_gpairs_s":
                          None if fp64_dropin is None else round(fp64_dropin, 3),
                      "speedup_vs_fp64_fused": round(value / fp64_fused, 3),

@@ -213,7 +213,7 @@ int vpm_sweep_records(int op, const void* records, int64_t n, int64_t target_beg
                       int ref_extra_4pi, double* out, double* out2, int precision,
                       void* workspace, size_t workspace_bytes, void* stream);
 
-/* ---- pair shards across GPUs (VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS, FP32C[_REFINED]) ----
+/* ---- pair shards across GPUs (VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS, every precision) --
  * The both-sides schedule of a self sum over n records split between ranks by tiles: rank r
  * runs the diagonal tiles [tile_begin, tile_end) and the diagonal pairs [pair_begin,
  * pair_end) of the plan every rank makes for n, over all n gathered records, and sums its

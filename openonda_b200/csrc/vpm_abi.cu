@@ -507,14 +507,31 @@ struct RotSweep {
     return 2 * m > kRotDiagSplit ? 2 * m : kRotDiagSplit;
   }
 
+  // The kernel of the operator's precision: rot_sweep_kernel (FP32 lanes) or
+  // rot64_sweep_kernel (FP64).
+  template <bool DIAG>
+  static const void* kernel_ptr() {
+    if constexpr (Op::kFP64)
+      return reinterpret_cast<const void*>(&rot64_sweep_kernel<Op, DIAG>);
+    else
+      return reinterpret_cast<const void*>(&rot_sweep_kernel<Op, DIAG>);
+  }
+  template <bool DIAG>
+  static void launch_kernel(unsigned grid, const RotArgs& a, cudaStream_t st) {
+    if constexpr (Op::kFP64)
+      rot64_sweep_kernel<Op, DIAG><<<grid, kRotThreads, kSmem, st>>>(a);
+    else
+      rot_sweep_kernel<Op, DIAG><<<grid, kRotThreads, kSmem, st>>>(a);
+  }
+
   // Shared-memory attributes and resident CTAs per SM, once per device (cached like the
   // one-sided sweeps' plans).
   static int prepare(int* occ) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    const void* ks = reinterpret_cast<const void*>(&rot_sweep_kernel<Op, false>);
-    const void* kd = reinterpret_cast<const void*>(&rot_sweep_kernel<Op, true>);
+    const void* ks = kernel_ptr<false>();
+    const void* kd = kernel_ptr<true>();
     const auto key = std::make_pair(ks, dev);
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_occ.find(key);
@@ -637,15 +654,13 @@ struct RotSweep {
       e = cudaEventRecord(ss->fork, st);
       if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord(fork)");
     } else {
-      rot_sweep_kernel<Op, true><<<nt * kRotDiagSplit, kRotThreads, kSmem, st>>>(
-          RotArgs{rec, n, nt, 0, acc});
+      launch_kernel<true>(unsigned(nt * kRotDiagSplit), RotArgs{rec, n, nt, 0, acc}, st);
       e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
     }
     for (int k0 = 1; k0 <= npairs; k0 += p.pairs) {
       const int m = (npairs - k0 + 1 < p.pairs) ? npairs - k0 + 1 : p.pairs;
-      rot_sweep_kernel<Op, false><<<m * nt, kRotThreads, kSmem, st>>>(
-          RotArgs{rec, n, nt, k0, acc});
+      launch_kernel<false>(unsigned(m * nt), RotArgs{rec, n, nt, k0, acc}, st);
       e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
     }
@@ -654,7 +669,7 @@ struct RotSweep {
       if (e != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent(fork)");
       RotArgs d{rec, n, nt, 0, acc};
       d.set0 = 2 * p.pairs;
-      rot_sweep_kernel<Op, true><<<nt * kRotDiagSplit, kRotThreads, kSmem, ss->stream>>>(d);
+      launch_kernel<true>(unsigned(nt * kRotDiagSplit), d, ss->stream);
       e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
       e = cudaEventRecord(ss->join, ss->stream);
@@ -680,15 +695,13 @@ struct RotSweep {
     if (t_end > t_begin) {
       RotArgs d{rec, n, nt, 0, acc};
       d.tile0 = t_begin;
-      rot_sweep_kernel<Op, true><<<(t_end - t_begin) * kRotDiagSplit, kRotThreads, kSmem, st>>>(
-          d);
+      launch_kernel<true>(unsigned((t_end - t_begin) * kRotDiagSplit), d, st);
       e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
     }
     for (int k0 = k_begin; k0 < k_end; k0 += p.pairs) {
       const int m = (k_end - k0 < p.pairs) ? k_end - k0 : p.pairs;
-      rot_sweep_kernel<Op, false><<<m * nt, kRotThreads, kSmem, st>>>(
-          RotArgs{rec, n, nt, k0, acc});
+      launch_kernel<false>(unsigned(m * nt), RotArgs{rec, n, nt, k0, acc}, st);
       e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_fail(e, "both-sides sweep launch");
     }
@@ -801,6 +814,7 @@ struct Ops {
   using VelStretchBoth = OpVelStretchBoth<REFINE, UC>;  // FP32 only
   using VelStretchBothAlt = OpVelStretchBoth<REFINE, UC, VPM_ROT_MINB_ALT>;
   using VelStretchBothSmall = OpVelStretchBoth<REFINE, UC, VPM_ROT_MINB_ALT, 2>;
+  using VelStretchBoth64 = OpVelStretchBoth64<UC>;  // FP64 only
   using VelBoth = OpVelBoth<REFINE, UC>;                // FP32 only
   using PseBoth = OpPseBoth<REFINE, UC>;                // FP32 only
   using LesStepBoth = OpLesStepBoth<REFINE, UC>;        // FP32 only
@@ -875,6 +889,9 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
           }
           return VPM_OK;
         }
+      } else {
+        if (RotSweep<typename O::VelStretchBoth64>::usable(m, n, mpb))
+          return RotSweep<typename O::VelStretchBoth64>::plan(n, p, mpb);
       }
       return Sweep<typename O::VelStretch, T>::plan(m, n, p, mpb);
     case VPM_OP_LES_STEP_SUMS:
@@ -1051,6 +1068,8 @@ int run(const Call& c) {
         else
           rc = Sweep<typename O::VelStretch, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n,
                                                         part, c.st);
+      } else if (p.pairs) {
+        rc = RotSweep<typename O::VelStretchBoth64>::launch(p, src, c.n, part, c.st);
       } else {
         rc = Sweep<typename O::VelStretch, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part,
                                                       c.st);
@@ -1496,16 +1515,16 @@ using namespace vpm;
 template <class T, bool REFINE, bool UC, class F>
 int with_fused_both(int64_t n, F&& f) {
   using O = Ops<T, REFINE, UC>;
+  Plan p;
+  int rc = plan_op<T, REFINE, UC>(VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS, n, n, &p);
+  if (rc) return rc;
+  if (!p.pairs)
+    return fail(VPM_ERR_ARG, "n = " + std::to_string(n) +
+                                 " does not take the both-sides schedule "
+                                 "(vpm_set_symmetric_min_n); shard the targets instead");
   if constexpr (LaneTraits<T>::kLanes != 2) {
-    return fail(VPM_ERR_ARG, "pair shards need an FP32-compensated precision");
+    return f(RotSweep<typename O::VelStretchBoth64>{}, p);
   } else {
-    Plan p;
-    int rc = plan_op<T, REFINE, UC>(VPM_OP_VELOCITY_AND_STRENGTH_GRADIENTS, n, n, &p);
-    if (rc) return rc;
-    if (!p.pairs)
-      return fail(VPM_ERR_ARG, "n = " + std::to_string(n) +
-                                   " does not take the both-sides schedule "
-                                   "(vpm_set_symmetric_min_n); shard the targets instead");
     if (p.variant == 2) return f(RotSweep<typename O::VelStretchBothSmall>{}, p);
     if (p.variant == 1) return f(RotSweep<typename O::VelStretchBothAlt>{}, p);
     return f(RotSweep<typename O::VelStretchBoth>{}, p);
@@ -1630,16 +1649,25 @@ int vpm_finalize_pairs_partial(int op, const double* rows, const void* records,
   if (!rows || !records || !out || !out2) return fail(VPM_ERR_ARG, "null pointer");
   if (reinterpret_cast<uintptr_t>(records) % 16 != 0)
     return fail(VPM_ERR_ALIGN, "records must be 16-byte aligned");
-  const int pr = precision & ~VPM_UNIFORM_CORE;
-  if (pr != VPM_FP32C && pr != VPM_FP32C_REFINED)
-    return fail(VPM_ERR_ARG, "pair shards need an FP32-compensated precision");
   int rc = check_arch();
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const Rec<float2>* tgt = static_cast<const Rec<float2>*>(records) + target_begin;
-  static_assert(OpVelStretchBoth<false, false>::NV == 9, "the fused sum's 9 values per row");
-  finalize_rows_kernel<float2, FIN_VELSTRETCH, 9><<<unsigned((m + 255) / 256), 256, 0, st>>>(
-      rows, m, tgt, out, out2);
+  static_assert(OpVelStretchBoth<false, false>::NV == 9 && OpVelStretchBoth64<false>::NV == 9,
+                "the fused sum's 9 values per row");
+  const unsigned blocks = unsigned((m + 255) / 256);
+  switch (precision & ~VPM_UNIFORM_CORE) {
+    case VPM_FP64:
+      finalize_rows_kernel<double, FIN_VELSTRETCH, 9><<<blocks, 256, 0, st>>>(
+          rows, m, static_cast<const Rec<double>*>(records) + target_begin, out, out2);
+      break;
+    case VPM_FP32C:
+    case VPM_FP32C_REFINED:
+      finalize_rows_kernel<float2, FIN_VELSTRETCH, 9><<<blocks, 256, 0, st>>>(
+          rows, m, static_cast<const Rec<float2>*>(records) + target_begin, out, out2);
+      break;
+    default:
+      return fail(VPM_ERR_ARG, "unknown precision " + std::to_string(precision));
+  }
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? VPM_OK : cuda_fail(e, "finalize launch");
 }

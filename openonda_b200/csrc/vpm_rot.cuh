@@ -155,8 +155,13 @@ __host__ __device__ constexpr int rot_tile() {
 // source-side sums of the first kSymFrom values, [kJBufs][kSymFrom][warps * 32].
 template <class Op>
 constexpr size_t rot_smem_bytes() {
-  return size_t(rot_tile<Op>()) * Op::NV * sizeof(double) +
-         size_t(Op::kJBufs) * Op::kSymFrom * kRotWarps * 32 * sizeof(float2);
+  if constexpr (Op::kFP64) {
+    // FP64 kernel: the warps' source-side sums of a batch only, [NV][warps * 32] doubles
+    return size_t(Op::NV) * kRotWarps * 32 * sizeof(double);
+  } else {
+    return size_t(rot_tile<Op>()) * Op::NV * sizeof(double) +
+           size_t(Op::kJBufs) * Op::kSymFrom * kRotWarps * 32 * sizeof(float2);
+  }
 }
 
 // The source a lane holds on the standard 64-byte record: position, core, strength.
@@ -205,6 +210,7 @@ struct RotStd {
   // Uniform cores: every record carries the same core, so the target's core, core^2 and
   // core^4 come from one record for all of a thread's packed lanes (one register pair each
   // instead of one per lane; the values are the same bits as the lanes' own)
+  static constexpr bool kFP64 = false;  // the FP32 kernel (rot_sweep_kernel)
   static constexpr bool kUniformCore = UC;
   __device__ __forceinline__ static void uniform_core(TgtT& t, const Record* rec) {
     const float sc = rec[0].s.x, s2 = sc * sc;
@@ -245,8 +251,12 @@ struct OpVelStretchBoth : RotStd<OpVelStretch<float2, REFINE, UC>, UC> {
   static constexpr int kJBufs = 2;     // double-buffered source-side sums
   __device__ __forceinline__ static constexpr bool short_fold(int v) { return v >= 3 && v < 6; }
   __device__ __forceinline__ static constexpr bool long_fold(int v) { return v < 3 || v >= 6; }
-  __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
-                                               const Src<V>& s) {
+  // one unordered pair for both particles, in any lane type (float2 here; double in the FP64
+  // operator below)
+  template <class W>
+  __device__ __forceinline__ static void pair2(const Tgt<W>& t, W* acc, W* jv,
+                                               const Src<W>& s) {
+    using V = W;
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
     V sg, s2;
     pair_core<UC>(t, s, sg, s2);
@@ -532,6 +542,7 @@ struct OpRhsVjpBoth {
   __device__ __forceinline__ static constexpr bool long_fold(int) { return false; }
   static constexpr int kSymFrom = NV;
   static constexpr int kJBufs = 2;
+  static constexpr bool kFP64 = false;
   static constexpr bool kUniformCore = false;
   __device__ __forceinline__ static void uniform_core(TgtT&, const Record*) {}
 
@@ -679,6 +690,45 @@ struct OpRhsVjpBoth {
   }
 };
 
+// The tile pair of this CTA: tiles I (targets) and J (sources), the accumulator sets its
+// target and source sides add into, and (DIAG) the part h of the diagonal tile's sources.
+// False for the CTAs past the middle diagonal's nt - k tile pairs.
+//
+// Two sets per diagonal pair: the first diagonal's target rows [0, nt - k) and the second's
+// source rows [nt - k, nt) share set 2q; the first's source rows [k, nt) and the second's
+// target rows [0, k) share set 2q + 1.  The row ranges in a set are disjoint and each tile
+// appears once per role, so every element still has one writer per launch.
+template <bool DIAG>
+__device__ __forceinline__ bool rot_block_pair(const RotArgs& a, int& I, int& J, int& set_i,
+                                               int& set_j, int& h) {
+  h = 0;
+  if (DIAG) {
+    const int t = blockIdx.x / kRotDiagSplit;
+    h = blockIdx.x - t * kRotDiagSplit;
+    I = J = a.tile0 + t;
+    set_i = a.set0 + h;  // each part into its own set: one writer per element
+    set_j = a.set0 + h;
+    return true;
+  }
+  const int q = blockIdx.x / a.nt, r = blockIdx.x - q * a.nt;
+  const int k = a.k0 + q, n1 = a.nt - k;
+  if (r < n1) {
+    I = r;
+    J = r + k;
+    set_i = 2 * q;
+    set_j = 2 * q + 1;
+    return true;
+  }
+  if (n1 > k) {
+    I = r - n1;
+    J = I + n1;
+    set_i = 2 * q + 1;
+    set_j = 2 * q;
+    return true;
+  }
+  return false;  // k == nt - k: the diagonal has only nt - k tile pairs
+}
+
 template <class Op, bool DIAG>
 __global__ void __launch_bounds__(kRotThreads, Op::kMinBlocks)
 rot_sweep_kernel(const RotArgs a) {
@@ -705,35 +755,8 @@ rot_sweep_kernel(const RotArgs a) {
   const Record* rec = static_cast<const Record*>(a.rec);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  int I, J, set_i, set_j;
-  int h = 0;  // DIAG: which part of the tile's sources this CTA takes
-  if (DIAG) {
-    const int t = blockIdx.x / kRotDiagSplit;
-    h = blockIdx.x - t * kRotDiagSplit;
-    I = J = a.tile0 + t;
-    set_i = a.set0 + h;  // each part into its own set: one writer per element
-    set_j = a.set0 + h;
-  } else {
-    const int q = blockIdx.x / a.nt, r = blockIdx.x - q * a.nt;
-    const int k = a.k0 + q, n1 = a.nt - k;
-    // Two sets per diagonal pair: the first diagonal's target rows [0, nt - k) and the
-    // second's source rows [nt - k, nt) share set 2q; the first's source rows [k, nt) and the
-    // second's target rows [0, k) share set 2q + 1.  The row ranges in a set are disjoint and
-    // each tile appears once per role, so every element still has one writer per launch.
-    if (r < n1) {
-      I = r;
-      J = r + k;
-      set_i = 2 * q;
-      set_j = 2 * q + 1;
-    } else if (n1 > k) {
-      I = r - n1;
-      J = I + n1;
-      set_i = 2 * q + 1;
-      set_j = 2 * q;
-    } else {
-      return;  // k == nt - k: the diagonal has only nt - k tile pairs
-    }
-  }
+  int I, J, set_i, set_j, h;
+  if (!rot_block_pair<DIAG>(a, I, J, set_i, set_j, h)) return;
   // sources: the whole tile J, or (DIAG) part h of the diagonal tile
   constexpr int TS = DIAG ? T / kRotDiagSplit : T;
   static_assert(TS % 32 == 0, "source ranges are whole batches");
@@ -876,6 +899,152 @@ rot_sweep_kernel(const RotArgs a) {
   for (int q = tid; q < T * NV; q += kRotThreads) {
     const int v = q / T, t = q - v * T;
     if (i0 + t < a.n) atomicAdd(&a.acc[(int64_t(set_i) * NV + v) * a.n + (i0 + t)], car[q]);
+  }
+}
+
+// ---- FP64: the fused sum on the both-sides schedule ------------------------------------------
+// The exact (FP64) form of the fused velocity + stretching sum with each unordered pair
+// evaluated once for both particles: the pair terms are OpVelStretchBoth::pair2 in double
+// (CUDA's rsqrt(double), as the one-sided FP64 sweep), and they differ from the one-sided
+// sweep's only in rounding (the triple product a_i . (r x a_j) in place of
+// r . ((a_j - a_i) x a_i)); the sums are FP64 throughout, so there are no windows and no
+// carries: each lane keeps R = 2 kP targets' sums in registers, and the source's sums travel
+// with it around the warp for the 32 steps of a batch.  Tiles, sets and launches are the
+// FP32 schedule's (rot_tile, rot_block_pair, the RotSweep planner).
+#ifndef VPM_ROT64_P
+#define VPM_ROT64_P 2  // R = 4 FP64 targets per lane, 512-particle tiles
+#endif
+#ifndef VPM_ROT64_MINB
+#define VPM_ROT64_MINB 2
+#endif
+
+template <bool UC>
+struct OpVelStretchBoth64 {
+  using V = double;
+  using Record = Rec<double>;
+  using OneSided = OpVelStretch<double, false, UC>;
+  using TgtT = Tgt<double>;
+  using SrcT = Src<double>;
+  static constexpr bool kFP64 = true;
+  static constexpr int NV = 9;
+  static constexpr int kP = VPM_ROT64_P;  // rot_tile: 64 kP warps = 32 R warps
+  static constexpr int kMinBlocks = VPM_ROT64_MINB;
+  static constexpr int kSymFrom = NV;
+  static constexpr bool kUniformCore = UC;
+  __device__ __forceinline__ static SrcT load(const Record* rec, int64_t j, int64_t n) {
+    if (j < n) return load_src<double>(rec[j]);
+    // far and without strength: r^2 = 1e220 stays finite and y^3 = 1e-330 underflows to 0,
+    // so the pair adds exactly nothing on either side
+    return SrcT{1e110, 1e110, 1e110, 1.0, 0.0, 0.0, 0.0, 0.0};
+  }
+  __device__ __forceinline__ static void shuffle(SrcT& c, int src_lane) {
+    c.x = __shfl_sync(0xffffffffu, c.x, src_lane);
+    c.y = __shfl_sync(0xffffffffu, c.y, src_lane);
+    c.z = __shfl_sync(0xffffffffu, c.z, src_lane);
+    if constexpr (!UC) c.s = __shfl_sync(0xffffffffu, c.s, src_lane);
+    c.ax = __shfl_sync(0xffffffffu, c.ax, src_lane);
+    c.ay = __shfl_sync(0xffffffffu, c.ay, src_lane);
+    c.az = __shfl_sync(0xffffffffu, c.az, src_lane);
+  }
+  __device__ __forceinline__ static void uniform_core(TgtT& t, const Record* rec) {
+    const double sc = rec[0].s, s2 = sc * sc;
+    t.sc = sc;
+    t.s2c = s2;
+    t.s4c = s2 * s2;
+  }
+  __device__ __forceinline__ static void pair2(const TgtT& t, double* acc, double* jv,
+                                               const SrcT& s) {
+    OpVelStretchBoth<false, UC>::pair2(t, acc, jv, s);
+  }
+};
+
+template <class Op, bool DIAG>
+__global__ void __launch_bounds__(kRotThreads, Op::kMinBlocks)
+rot64_sweep_kernel(const RotArgs a) {
+  using Record = typename Op::Record;
+  constexpr int NV = Op::NV;
+  constexpr int R = 2 * Op::kP;  // targets per lane
+  constexpr int T = rot_tile<Op>();
+  constexpr int WT = kRotWarps * 32;
+  static_assert(T == R * WT, "a tile is the CTA's lanes times their targets");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  double* jbuf = reinterpret_cast<double*>(smem_raw);  // [NV][WT]
+  const Record* rec = static_cast<const Record*>(a.rec);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  int I, J, set_i, set_j, h;
+  if (!rot_block_pair<DIAG>(a, I, J, set_i, set_j, h)) return;
+  constexpr int TS = DIAG ? T / kRotDiagSplit : T;
+  static_assert(TS % 32 == 0, "source ranges are whole batches");
+  const int64_t i0 = int64_t(I) * T, j0 = int64_t(J) * T + int64_t(h) * TS;
+  const int cnt = int((a.n - j0 < TS) ? (a.n - j0 > 0 ? a.n - j0 : 0) : TS);
+
+  // this lane's targets: warp * 32 R + 32 r + lane
+  typename Op::TgtT tg[R];
+  int64_t ti[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    ti[r] = i0 + warp * 32 * R + r * 32 + lane;
+    const Record* rp = rec + (ti[r] < a.n ? ti[r] : a.n - 1);
+    tg[r] = make_tgt(&rp);
+    if constexpr (Op::kUniformCore) Op::uniform_core(tg[r], rec);
+  }
+  double acc[R][NV];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[r][v] = 0.0;
+
+  const int nb = (cnt + 31) / 32;
+  const int src_lane = (lane + 1) & 31;
+  typename Op::SrcT nxt = Op::load(rec, j0 + lane, j0 + cnt);
+  for (int b = 0; b < nb; ++b) {
+    typename Op::SrcT cur = nxt;  // the source this lane holds at step 0
+    if (b + 1 < nb) nxt = Op::load(rec, j0 + (b + 1) * 32 + lane, j0 + cnt);
+    double jv[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) jv[v] = 0.0;
+#pragma unroll 2
+    for (int st = 0; st < 32; ++st) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if constexpr (DIAG)
+          Op::OneSided::pair(tg[r], acc[r], cur, nullptr, 0);
+        else
+          Op::pair2(tg[r], acc[r], jv, cur);
+      }
+      // the source and its sums one lane down; after 32 steps both are back in their lane
+      Op::shuffle(cur, src_lane);
+      if constexpr (!DIAG) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) jv[v] = __shfl_sync(0xffffffffu, jv[v], src_lane);
+      }
+    }
+    if constexpr (!DIAG) {
+      // the warps' sums of source b * 32 + lane, added over the warps in a fixed order
+#pragma unroll
+      for (int v = 0; v < NV; ++v) jbuf[v * WT + warp * 32 + lane] = jv[v];
+      __syncthreads();
+      const int nsrc = (cnt - b * 32 < 32) ? cnt - b * 32 : 32;
+      for (int q = tid; q < 32 * NV; q += kRotThreads) {
+        const int v = q >> 5, jj = q & 31;
+        if (jj >= nsrc) continue;
+        double sum = 0.0;
+#pragma unroll
+        for (int w = 0; w < kRotWarps; ++w) sum += jbuf[v * WT + w * 32 + jj];
+        // the only writer of this element in this launch (non-returning, fixed order)
+        atomicAdd(&a.acc[(int64_t(set_j) * NV + v) * a.n + (j0 + b * 32 + jj)], -sum);
+      }
+      __syncthreads();  // jbuf is read before the next batch writes it
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    if (ti[r] < a.n) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+        atomicAdd(&a.acc[(int64_t(set_i) * NV + v) * a.n + ti[r]], acc[r][v]);
+    }
   }
 }
 

@@ -7,7 +7,7 @@ Each rank owns a contiguous shard of the particles.  One sweep is:
 2. all-gather the records of every shard (NCCL over NVLink -- 64 MB at N = 2^20),
 3. either (target shards) sweep the rank's own targets against all gathered sources with
    ``vpm_sweep_records``; nothing else crosses GPUs,
-   or (pair shards, FP32c sizes that take the both-sides schedule) run the rank's share of
+   or (pair shards, sizes that take the both-sides schedule) run the rank's share of
    that schedule's tiles and diagonal pairs over all particles with
    ``vpm_sweep_pairs_partial``, reduce-scatter the (n, 9) FP64 partial sums by row ranges
    (72 MB at N = 2^20) and finalize the rank's own rows with
@@ -199,8 +199,6 @@ class ShardedVelocityStretching:
             self.kernel_launches_per_call = 1 + self.sweep_launches
 
     def _pair_plan(self, lib):
-        if self.precision not in ("fp32c", "fp32c_refined"):
-            return None
         layout = pairs_layout(self.n, self.precision)
         if layout is None:
             return None  # below the both-sides size: target shards

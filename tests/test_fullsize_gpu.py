@@ -55,6 +55,27 @@ def test_fp64_windows_vs_oracle(cloud, fp64):
         assert eg <= FP64_TOL_2_20, (t0, eg)
 
 
+def test_fp64_both_sides_against_the_one_sided_sweep(cloud, fp64):
+    """At this size the fused FP64 sum takes the both-sides schedule (each unordered pair once
+    for both particles, FP64 register sums); the one-sided FP64 sweep over the same field
+    differs from it only by rounding (summation order, and the triple product of the
+    stretching term, which the both-sides form takes as the reference does)."""
+    from openonda_b200 import kernels
+
+    _, x, a, s, _ = cloud
+    assert kernels.sweep_launches("velocity_and_strength_gradients", "fp64", N, N) > 2
+    prev = kernels.set_symmetric_min_n(1 << 40)
+    try:
+        assert kernels.sweep_launches("velocity_and_strength_gradients", "fp64", N, N) == 2
+        one = kernels.velocity_and_strength_gradients(x, a, s, precision="fp64")
+    finally:
+        kernels.set_symmetric_min_n(prev)
+    for k in range(2):
+        e = normwise(fp64[k].cpu().numpy(), one[k].cpu().numpy())
+        print(f"k={k}: both-sides vs one-sided FP64 {e:.2e}")
+        assert e <= FP64_TOL_2_20, (k, e)
+
+
 def test_fp32c_vs_fp64_full_size(cloud):
     from openonda_b200 import kernels
 
