@@ -815,6 +815,8 @@ struct Ops {
   using VelStretchBothAlt = OpVelStretchBoth<REFINE, UC, VPM_ROT_MINB_ALT>;
   using VelStretchBothSmall = OpVelStretchBoth<REFINE, UC, VPM_ROT_MINB_ALT, 2>;
   using VelStretchBoth64 = OpVelStretchBoth64<UC>;  // FP64 only
+  using VelBoth64 = OpVelBoth64<UC>;                // FP64 only
+  using PseBoth64 = OpPseBoth64<UC>;                // FP64 only
   using VelBoth = OpVelBoth<REFINE, UC>;                // FP32 only
   using PseBoth = OpPseBoth<REFINE, UC>;                // FP32 only
   using LesStepBoth = OpLesStepBoth<REFINE, UC>;        // FP32 only
@@ -835,6 +837,9 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
       if constexpr (LaneTraits<T>::kLanes == 2) {
         if (RotSweep<typename O::VelBoth>::usable(m, n, mpb))
           return RotSweep<typename O::VelBoth>::plan(n, p, mpb);
+      } else {
+        if (RotSweep<typename O::VelBoth64>::usable(m, n, mpb))
+          return RotSweep<typename O::VelBoth64>::plan(n, p, mpb);
       }
       return Sweep<typename O::Vel, T>::plan(m, n, p, mpb);
     case VPM_OP_TOTAL_HELICITY:
@@ -849,6 +854,9 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
       if constexpr (LaneTraits<T>::kLanes == 2) {
         if (RotSweep<typename O::PseBoth>::usable(m, n, mpb))
           return RotSweep<typename O::PseBoth>::plan(n, p, mpb);
+      } else {
+        if (RotSweep<typename O::PseBoth64>::usable(m, n, mpb))
+          return RotSweep<typename O::PseBoth64>::plan(n, p, mpb);
       }
       return Sweep<typename O::Pse, T>::plan(m, n, p, mpb);
     case VPM_OP_TOTAL_KINETIC_ENERGY:
@@ -1026,9 +1034,11 @@ int run(const Call& c) {
   switch (c.op) {
     case VPM_OP_SELFINDUCED_VELOCITY:
       rc = VPM_OK;
-      if constexpr (LaneTraits<T>::kLanes == 2) {
-        if (p.pairs)  // m == n: the targets are all the records (tgt_begin == 0)
+      if (p.pairs) {  // m == n: the targets are all the records (tgt_begin == 0)
+        if constexpr (LaneTraits<T>::kLanes == 2)
           rc = RotSweep<typename O::VelBoth>::launch(p, src, c.n, part, c.st);
+        else
+          rc = RotSweep<typename O::VelBoth64>::launch(p, src, c.n, part, c.st);
       }
       if (!p.pairs)
         rc = Sweep<typename O::Vel, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
@@ -1049,9 +1059,11 @@ int run(const Call& c) {
       return rc;
     case VPM_OP_STRENGTH_GRADIENTS_PSE:
       rc = VPM_OK;
-      if constexpr (LaneTraits<T>::kLanes == 2) {
-        if (p.pairs)
+      if (p.pairs) {
+        if constexpr (LaneTraits<T>::kLanes == 2)
           rc = RotSweep<typename O::PseBoth>::launch(p, src, c.n, part, c.st);
+        else
+          rc = RotSweep<typename O::PseBoth64>::launch(p, src, c.n, part, c.st);
       }
       if (!p.pairs)
         rc = Sweep<typename O::Pse, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);

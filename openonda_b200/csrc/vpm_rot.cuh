@@ -318,8 +318,10 @@ struct OpVelBoth : RotStd<OpVel<float2, REFINE, UC>, UC> {
   static constexpr int kTgtWindow = 32;
   static constexpr int kSymFrom = NV;
   static constexpr int kJBufs = 2;
-  __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
-                                               const Src<V>& s) {
+  template <class W>
+  __device__ __forceinline__ static void pair2(const Tgt<W>& t, W* acc, W* jv,
+                                               const Src<W>& s) {
+    using V = W;
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
     V sg, s2;
     pair_core<UC>(t, s, sg, s2);
@@ -363,8 +365,10 @@ struct OpPseBoth : RotStd<OpPse<float2, REFINE, UC>, UC> {
   static constexpr int kTgtWindow = 32;
   static constexpr int kSymFrom = NV;
   static constexpr int kJBufs = 2;
-  __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
-                                               const Src<V>& s) {
+  template <class W>
+  __device__ __forceinline__ static void pair2(const Tgt<W>& t, W* acc, W* jv,
+                                               const Src<W>& s) {
+    using V = W;
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
     V sg, s2;
     pair_core<UC>(t, s, sg, s2);
@@ -903,8 +907,9 @@ rot_sweep_kernel(const RotArgs a) {
 }
 
 // ---- FP64: the fused sum on the both-sides schedule ------------------------------------------
-// The exact (FP64) form of the fused velocity + stretching sum with each unordered pair
-// evaluated once for both particles: the pair terms are OpVelStretchBoth::pair2 in double
+// The exact (FP64) form of the fused velocity + stretching sum (and of the velocity and PSE
+// sums) with each unordered pair evaluated once for both particles: the pair terms are the
+// FP32 operators' pair2 in double
 // (CUDA's rsqrt(double), as the one-sided FP64 sweep), and they differ from the one-sided
 // sweep's only in rounding (the triple product a_i . (r x a_j) in place of
 // r . ((a_j - a_i) x a_i)); the sums are FP64 throughout, so there are no windows and no
@@ -918,17 +923,19 @@ rot_sweep_kernel(const RotArgs a) {
 #define VPM_ROT64_MINB 2
 #endif
 
-template <bool UC>
-struct OpVelStretchBoth64 {
+// Both32: the FP32 both-sides operator whose pair2 (a template in the lane type) gives the
+// pair terms; OneSided64: the one-sided FP64 operator of the diagonal tiles.
+template <class Both32, class OneSided64, bool UC, int MINB = VPM_ROT64_MINB>
+struct OpBoth64 {
   using V = double;
   using Record = Rec<double>;
-  using OneSided = OpVelStretch<double, false, UC>;
+  using OneSided = OneSided64;
   using TgtT = Tgt<double>;
   using SrcT = Src<double>;
   static constexpr bool kFP64 = true;
-  static constexpr int NV = 9;
+  static constexpr int NV = Both32::NV;
   static constexpr int kP = VPM_ROT64_P;  // rot_tile: 64 kP warps = 32 R warps
-  static constexpr int kMinBlocks = VPM_ROT64_MINB;
+  static constexpr int kMinBlocks = MINB;
   static constexpr int kSymFrom = NV;
   static constexpr bool kUniformCore = UC;
   __device__ __forceinline__ static SrcT load(const Record* rec, int64_t j, int64_t n) {
@@ -954,9 +961,17 @@ struct OpVelStretchBoth64 {
   }
   __device__ __forceinline__ static void pair2(const TgtT& t, double* acc, double* jv,
                                                const SrcT& s) {
-    OpVelStretchBoth<false, UC>::pair2(t, acc, jv, s);
+    Both32::pair2(t, acc, jv, s);
   }
 };
+template <bool UC>
+using OpVelStretchBoth64 =
+    OpBoth64<OpVelStretchBoth<false, UC>, OpVelStretch<double, false, UC>, UC>;
+// the three-sum operators fit three CTAs per SM
+template <bool UC>
+using OpVelBoth64 = OpBoth64<OpVelBoth<false, UC>, OpVel<double, false, UC>, UC, 3>;
+template <bool UC>
+using OpPseBoth64 = OpBoth64<OpPseBoth<false, UC>, OpPse<double, false, UC>, UC, 3>;
 
 template <class Op, bool DIAG>
 __global__ void __launch_bounds__(kRotThreads, Op::kMinBlocks)

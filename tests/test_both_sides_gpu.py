@@ -123,6 +123,43 @@ def test_small_tile_build_vs_fp64(uniform_core):
     assert kernels.device_errors() == 0
 
 
+@pytest.mark.parametrize("uniform_core", [False, True])
+def test_fp64_both_sides_vs_oracle(uniform_core):
+    """FP64 self sums at N = 30000 take the both-sides schedule (rot64_sweep_kernel: the
+    fused sum, the velocity and PSE); against the oracle (the reference's GPU semantics in
+    FP64 C) they hold the reference's 1e-12, and they repeat bit for bit."""
+    import oracle
+    from openonda_b200 import kernels
+
+    n = 30000
+    f = _field(n, 29, False)
+    if uniform_core:
+        f.radii[:] = f.radii[0]
+    x, a, s = (torch.from_numpy(np.ascontiguousarray(z)).cuda()
+               for z in (f.positions, f.strengths, f.radii))
+    nu = torch.from_numpy(np.ascontiguousarray(f.viscosities)).cuda()
+    for op in ("velocity_and_strength_gradients", "selfinduced_velocity",
+               "strength_gradients_pse"):
+        assert kernels.sweep_launches(op, "fp64", n, n) > 2, op
+    u, g = kernels.velocity_and_strength_gradients(x, a, s, precision="fp64",
+                                                   uniform_core=uniform_core)
+    v = kernels.selfinduced_velocity(x, a, s, precision="fp64", uniform_core=uniform_core)
+    p = kernels.strength_gradients_pse(x, a, s, nu, precision="fp64", uniform_core=uniform_core)
+    ru = oracle.gpu.get_selfinduced_velocity(f.positions, f.strengths, f.radii)
+    rg = oracle.gpu.get_strength_gradients(f.positions, f.strengths, f.radii)
+    rp = oracle.gpu.get_strength_gradients_PSE(f.positions, f.strengths, f.radii,
+                                               f.viscosities)
+    for name, got, ref in (("velocity", u, ru), ("stretching", g, rg), ("velocity only", v, ru),
+                           ("pse", p, rp)):
+        e = normwise(got.cpu().numpy(), ref)
+        print(f"uc={uniform_core} {name}: {e:.2e}")
+        assert e <= 1e-12, (name, e)
+    again = kernels.strength_gradients_pse(x, a, s, nu, precision="fp64",
+                                           uniform_core=uniform_core)
+    assert torch.equal(p, again)
+    assert kernels.device_errors() == 0
+
+
 def test_both_sides_is_deterministic(both_sides_always):
     from openonda_b200 import kernels
 
@@ -203,15 +240,22 @@ def test_velocity_and_pse_both_sides_vs_fp64(op, n, ring, uniform_core):
 
 
 def test_helicity_and_shards_stay_one_sided(both_sides_always):
-    """Only whole-set self sums of the FP32c precisions take the both-sides sweep."""
+    """Only whole-set self sums take the both-sides sweep: in FP32c the fused, velocity, PSE
+    and LES step sums and the adjoint, in FP64 the fused, velocity and PSE sums; the
+    diagnostics, the stretching-only sum and target shards (m < n) stay one-sided."""
     from openonda_b200 import kernels
 
     n = 4096
     assert kernels.sweep_launches("selfinduced_velocity", "fp32c", n, n) > 2
     assert kernels.sweep_launches("total_helicity", "fp32c", n, n) == 2
     assert kernels.sweep_launches("selfinduced_velocity", "fp32c", 1000, n) == 2
-    assert kernels.sweep_launches("strength_gradients_pse", "fp64", n, n) == 2
     assert kernels.sweep_launches("strength_gradients_pse", "fp32c", n, n) > 2
+    for prec in ("fp32c", "fp64"):
+        assert kernels.sweep_launches("strength_gradients", prec, n, n) == 2
+    for op in ("velocity_and_strength_gradients", "selfinduced_velocity",
+               "strength_gradients_pse"):
+        assert kernels.sweep_launches(op, "fp64", n, n) > 2
+        assert kernels.sweep_launches(op, "fp64", 1000, n) == 2
 
 
 @pytest.mark.parametrize("n,ring", [(ONE_PAST_TILE, False), (1000, False), (3001, False),
