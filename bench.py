@@ -453,7 +453,7 @@ def main():
     fp64_fused = float(n) * n / (t64 / args.fp64_steps) / 1e9
     err_u = max_over_ranks(normwise(u32, u64))
     err_g = max_over_ranks(normwise(g32, g64))
-    fp64_dropin = fp64_one_sided = None
+    fp64_dropin = fp64_one_sided = fp64_dropin_shipped = None
     if world == 1:
         xa = torch.from_numpy(x_h).to(dev)
         aa = torch.from_numpy(a_h).to(dev)
@@ -463,17 +463,21 @@ def main():
             return (kernels.selfinduced_velocity(xa, aa, sa, precision="fp64"),
                     kernels.strength_gradients(xa, aa, sa, precision="fp64"))
 
+        # the drop-in as shipped (its velocity sweep takes the both-sides schedule here)
         tdi, _, _ = timed(dropin, 1, 1)
-        fp64_dropin = float(n) * n / tdi / 1e9
-        # the plain FP64 kernel: the fused sum one-sided (each ordered pair evaluated for its
-        # target only), as the reference's kernels evaluate it
+        fp64_dropin_shipped = float(n) * n / tdi / 1e9
+        # the plain FP64 kernels, one-sided (each ordered pair evaluated for its target only)
+        # as the reference's kernels evaluate them: the fused sum, and the two separate
+        # sweeps the reference calls
         prev = kernels.set_symmetric_min_n(1 << 40)
         try:
             tos, _, _ = timed(lambda: kernels.velocity_and_strength_gradients(
                 xa, aa, sa, precision="fp64"), 1, 1)
+            tdp, _, _ = timed(dropin, 1, 1)
         finally:
             kernels.set_symmetric_min_n(prev)
         fp64_one_sided = float(n) * n / tos / 1e9
+        fp64_dropin = float(n) * n / tdp / 1e9
         del xa, aa, sa
 
     # ---- the reference's own Numba-CUDA kernels (ParticlesPhysicsCuda.py, unmodified, from
@@ -599,7 +603,13 @@ def main():
                          None if fp64_dropin is None else round(fp64_dropin, 3),
                      "speedup_vs_fp64_fused": round(value / fp64_fused, 3),
                      "speedup_vs_fp64_dropin":
-                         None if fp64_dropin is None else round(value / fp64_dropin, 3)},
+                         None if fp64_dropin is None else round(value / fp64_dropin, 3),
+                     "dropin_shipped_gpairs_s":
+                         None if fp64_dropin_shipped is None
+                         else round(fp64_dropin_shipped, 3),
+                     "speedup_vs_fp64_dropin_shipped":
+                         None if fp64_dropin_shipped is None
+                         else round(value / fp64_dropin_shipped, 3)},
             "rel_err_vs_fp64": {"velocity": err_u, "stretching": err_g},
             "reference_gpu": ref_gpu,
             "reference_cpu": ref_cpu,

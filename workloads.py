@@ -219,15 +219,19 @@ def config3(args):
             res[prec] = n * n / (best / 1e3) / 1e9
         path = ("both-sides" if kernels.sweep_launches("velocity_and_strength_gradients",
                                                         "fp32c", n, n) > 2 else "one-sided")
+        path64 = ("both-sides" if kernels.sweep_launches("velocity_and_strength_gradients",
+                                                          "fp64", n, n) > 2 else "one-sided")
         ops, rsq = _FUSED_OPS[path]
+        ops64 = _FUSED_OPS[path64][0]  # the FP64 kernels execute the same pair terms
         r32 = res["fp32c"] * 1e9
         _emit({"config": "config3", "n": n, "fp32c_gpairs_s": round(res["fp32c"], 1),
                "fp64_gpairs_s": round(res["fp64"], 1),
                "speedup": round(res["fp32c"] / res["fp64"], 2), "fp32c_path": path,
+               "fp64_path": path64,
                "fp32_pipe_frac": round(r32 * ops / peaks["ffma"], 3),
                "fp32_pipe_frac_of_packed": round(r32 * ops / peaks["ffma2"], 3),
                "sfu_frac": round(r32 * rsq / peaks["mufu"], 3),
-               "fp64_pipe_frac_excl_rsqrt": round(res["fp64"] * 1e9 * 38.0 / peaks["dfma"], 3),
+               "fp64_pipe_frac_excl_rsqrt": round(res["fp64"] * 1e9 * ops64 / peaks["dfma"], 3),
                "rel_err_velocity": _rel(out["fp32c"][0], out["fp64"][0]),
                "rel_err_stretching": _rel(out["fp32c"][1], out["fp64"][1])})
 
