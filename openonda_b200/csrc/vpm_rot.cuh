@@ -1,6 +1,6 @@
-// vpm_rot.cuh -- both-sides sweeps of the FP32-compensated self sums (fused velocity +
-// stretching, velocity, PSE, the LES step sums, the adjoint of (u, S)), with the source side
-// carried around the warp in registers.
+// vpm_rot.cuh -- both-sides sweeps of the self sums (FP32-compensated: fused velocity +
+// stretching, velocity, PSE, the LES step sums, the adjoint of (u, S); FP64: the fused,
+// velocity and PSE sums), with the source side carried around the warp in registers.
 //
 // The pair terms of (i <- j) and (j <- i) share r^2, the core, the rsqrt and the kernel
 // values.  Seen from particle j, with r = x_i - x_j as computed for target i:
@@ -33,10 +33,12 @@
 // tile's sources each and add into sets 0 .. kRotDiagSplit - 1.  The finalize pass sums the
 // max(2m, kRotDiagSplit) sets in order.
 //
-// Accumulation: target side in FP32 per batch of 32 sources, folded into FP64 carries held in
-// shared memory; source side in FP32 over windows of kSrcWindow steps (each half of the
-// packed accumulator sums kSrcWindow kP terms), the windows of a batch added in FP32 in
-// shared memory, then both halves in FP64 across warps and tile pairs.
+// Accumulation (FP32 kernel): target side in FP32 over windows of 16 to 64 steps per value
+// (kTgtWindow, kTgtWindowShort, kTgtWindowLong), folded into FP64 carries held in shared
+// memory; source side in FP32 over windows of kSrcWindow steps (each half of the packed
+// accumulator sums kSrcWindow kP terms), the windows of a batch added in FP32 in shared
+// memory, then both halves in FP64 across warps and tile pairs.  The FP64 kernel
+// (rot64_sweep_kernel, at the end) keeps every sum in FP64 registers.
 #pragma once
 
 #include "vpm_adjoint.cuh"
