@@ -779,6 +779,9 @@ rot_sweep_kernel(const RotArgs a) {
     lt[2 * p] = warp * 64 * P + p * 64 + lane;
     lt[2 * p + 1] = lt[2 * p] + 32;
     const int64_t t0 = i0 + lt[2 * p], t1 = i0 + lt[2 * p + 1];
+    // targets past n (a copy of the last record) occur only in the diagonal tiles: a tile
+    // pair has I < J <= nt - 1, so its target tile is whole; the diagonal tiles are one-sided,
+    // so those copies add to no source, and their own sums are never stored
     const Record* recs[2] = {rec + (t0 < a.n ? t0 : a.n - 1), rec + (t1 < a.n ? t1 : a.n - 1)};
     tg[p] = Op::target(recs);
     if constexpr (Op::kUniformCore) Op::uniform_core(tg[p], rec);
@@ -1002,6 +1005,7 @@ rot64_sweep_kernel(const RotArgs a) {
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     ti[r] = i0 + warp * 32 * R + r * 32 + lane;
+    // past n only in the (one-sided) diagonal tiles, as in rot_sweep_kernel
     const Record* rp = rec + (ti[r] < a.n ? ti[r] : a.n - 1);
     tg[r] = make_tgt(&rp);
     if constexpr (Op::kUniformCore) Op::uniform_core(tg[r], rec);
