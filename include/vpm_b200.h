@@ -157,12 +157,17 @@ int vpm_velocity_and_strength_gradients(const double* positions, const double* s
                                         size_t workspace_bytes, void* stream);
 
 /* FP32-compensated self sums of velocity + stretching, velocity alone, PSE and the LES step
- * sums, and the adjoint of (u, S [+ P]) (vpm_velocity_and_strength_gradients,
- * vpm_selfinduced_velocity, vpm_strength_gradients_pse, vpm_les_step_sums, vpm_rhs_vjp, and
- * vpm_sweep_records over all records) with n >= this value evaluate each unordered pair once
- * for both particles (deterministic tile-pair schedule, about n / (2 T m) launches for tiles
- * of T = 512 or 768 particles and m diagonal pairs per launch).  Sets the threshold and
- * returns the previous one (default 24576).  No counterpart in the reference. */
+ * sums, the adjoint of (u, S [+ P]), and the FP64 self sums of velocity + stretching, velocity
+ * alone and PSE (vpm_velocity_and_strength_gradients, vpm_selfinduced_velocity,
+ * vpm_strength_gradients_pse, vpm_les_step_sums, vpm_rhs_vjp, and vpm_sweep_records over all
+ * records) with n >= this value evaluate each unordered pair once for both particles
+ * (deterministic tile-pair schedule, about n / (2 T m) launches for tiles of T = 512 or 768
+ * particles and m diagonal pairs per launch).  Where those launches are short (up to ~150000
+ * particles), the diagonal tiles run on a second stream of the library's, forked from and
+ * joined to the caller's stream by events inside the call, so stream order and CUDA-graph
+ * capture see one call as before; that stream is created by the first such call in a context
+ * (make it before any stream capture).  Sets the threshold and returns the previous one
+ * (default 24576).  No counterpart in the reference. */
 int64_t vpm_set_symmetric_min_n(int64_t n);
 /* Kernel launches of one sweep of `op` (sweep and finalize, not the packing of the inputs)
  * for m targets and n sources under the current plan; -1 on error. */
@@ -348,7 +353,9 @@ int vpm_lattice_cylindrical(double particle_distance, double radius, double heig
  * library (reserved on every GPU that loads it), so n <= VPM_NOALLOC_MAX_N (larger n returns
  * VPM_ERR_ARG).  All calls share that array: calls that overlap on the GPU race.  The array
  * has one address per CUDA context; the first call in a context (per device) looks that
- * address up, so make it before any stream capture.  If a sweep's bounded wait gives up
+ * address up (and, for sizes whose sweep runs its diagonal tiles on a second stream, creates
+ * that stream and its two events), so make it before any stream capture.  If a sweep's
+ * bounded wait gives up
  * (bit 0 of the vpm_device_errors word), the output is built from the previous call's
  * partial sums: check the device error word where that matters. */
 int vpm_selfinduced_velocity_noalloc(const double* positions, const double* strengths,
