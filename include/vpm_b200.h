@@ -158,7 +158,7 @@ int vpm_velocity_and_strength_gradients(const double* positions, const double* s
 
 /* FP32-compensated self sums of velocity + stretching, velocity alone, PSE and the LES step
  * sums, the adjoint of (u, S [+ P]), and the FP64 self sums of velocity + stretching, velocity
- * alone and PSE (vpm_velocity_and_strength_gradients, vpm_selfinduced_velocity,
+ * alone, PSE and the LES step (vpm_velocity_and_strength_gradients, vpm_selfinduced_velocity,
  * vpm_strength_gradients_pse, vpm_les_step_sums, vpm_rhs_vjp, and vpm_sweep_records over all
  * records) with n >= this value evaluate each unordered pair once for both particles
  * (deterministic tile-pair schedule, about n / (2 T m) launches for tiles of T = 512 or 768

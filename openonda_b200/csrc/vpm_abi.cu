@@ -817,6 +817,7 @@ struct Ops {
   using VelStretchBoth64 = OpVelStretchBoth64<UC>;  // FP64 only
   using VelBoth64 = OpVelBoth64<UC>;                // FP64 only
   using PseBoth64 = OpPseBoth64<UC>;                // FP64 only
+  using LesStepBoth64 = OpLesStepBoth64<UC>;        // FP64 only
   using VelBoth = OpVelBoth<REFINE, UC>;                // FP32 only
   using PseBoth = OpPseBoth<REFINE, UC>;                // FP32 only
   using LesStepBoth = OpLesStepBoth<REFINE, UC>;        // FP32 only
@@ -906,6 +907,9 @@ int plan_op(int op, int64_t m, int64_t n, Plan* p, size_t mpb = kMaxPartialBytes
       if constexpr (LaneTraits<T>::kLanes == 2) {
         if (RotSweep<typename O::LesStepBoth>::usable(m, n, mpb))
           return RotSweep<typename O::LesStepBoth>::plan(n, p, mpb);
+      } else {
+        if (RotSweep<typename O::LesStepBoth64>::usable(m, n, mpb))
+          return RotSweep<typename O::LesStepBoth64>::plan(n, p, mpb);
       }
       return Sweep<typename O::LesStep, T>::plan(m, n, p, mpb);
     case VPM_OP_RHS_VJP:
@@ -1093,9 +1097,11 @@ int run(const Call& c) {
     case VPM_OP_LES_STEP_SUMS: {
       using Op = typename O::LesStep;
       rc = VPM_OK;
-      if constexpr (LaneTraits<T>::kLanes == 2) {
-        if (p.pairs)
+      if (p.pairs) {
+        if constexpr (LaneTraits<T>::kLanes == 2)
           rc = RotSweep<typename O::LesStepBoth>::launch(p, src, c.n, part, c.st);
+        else
+          rc = RotSweep<typename O::LesStepBoth64>::launch(p, src, c.n, part, c.st);
       }
       if (!p.pairs) rc = Sweep<Op, T>::launch(p, tgt, c.m, c.tgt_begin, src, c.n, part, c.st);
       if (rc) return rc;
@@ -1105,6 +1111,7 @@ int run(const Call& c) {
         // both sides: the per-target scalar sum_j ke (a_i . a_j) (value 12), taken once per
         // unordered pair, so the sum is doubled
         constexpr int NVB = O::LesStepBoth::NV;
+        static_assert(O::LesStepBoth64::NV == NVB, "one row layout for both precisions");
         rc = finalize_vec<T, FIN_LES, NVB>(part, p.splits, c.m, tgt, c.out, c.out2, c.st,
                                            c.out3);
         if (rc) return rc;

@@ -158,8 +158,8 @@ __host__ __device__ constexpr int rot_tile() {
 template <class Op>
 constexpr size_t rot_smem_bytes() {
   if constexpr (Op::kFP64) {
-    // FP64 kernel: the warps' source-side sums of a batch only, [NV][warps * 32] doubles
-    return size_t(Op::NV) * kRotWarps * 32 * sizeof(double);
+    // FP64 kernel: the warps' source-side sums of a batch only, [kSymFrom][warps * 32]
+    return size_t(Op::kSymFrom) * kRotWarps * 32 * sizeof(double);
   } else {
     return size_t(rot_tile<Op>()) * Op::NV * sizeof(double) +
            size_t(Op::kJBufs) * Op::kSymFrom * kRotWarps * 32 * sizeof(float2);
@@ -213,6 +213,7 @@ struct RotStd {
   // core^4 come from one record for all of a thread's packed lanes (one register pair each
   // instead of one per lane; the values are the same bits as the lanes' own)
   static constexpr bool kFP64 = false;  // the FP32 kernel (rot_sweep_kernel)
+  static constexpr bool kCustomDiag = false;  // the diagonal tiles take OneSided::pair
   static constexpr bool kUniformCore = UC;
   __device__ __forceinline__ static void uniform_core(TgtT& t, const Record* rec) {
     const float sc = rec[0].s.x, s2 = sc * sc;
@@ -402,6 +403,15 @@ struct OpPseBoth : RotStd<OpPse<float2, REFINE, UC>, UC> {
 // sum_j ke (a_i . a_j) (value 12) in place of the three components of E_i.  65 FP32 lane-ops
 // per unordered pair with uniform cores, about 80 without (one-sided: 2 x 52, 2 x 56).  Two
 // CTAs per SM, step loop unrolled 2.
+// v where a > thr, else 0 (per packed lane)
+__device__ __forceinline__ float2 keep_if_gt(float2 a, double thr, float2 v) {
+  const float t = float(thr);
+  return make_float2(a.x > t ? v.x : 0.f, a.y > t ? v.y : 0.f);
+}
+__device__ __forceinline__ double keep_if_gt(double a, double thr, double v) {
+  return a > thr ? v : 0.0;
+}
+
 template <bool REFINE, bool UC>
 struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
   using V = float2;
@@ -420,8 +430,11 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
   // three resident CTAs fit the shared memory only with one buffer of source-side sums
   static constexpr int kJBufs = VPM_ROT15_MINB >= 3 ? 1 : 2;
   __device__ __forceinline__ static constexpr bool carried(int v) { return v < kSymFrom; }
-  __device__ __forceinline__ static void pair2(const Tgt<V>& t, V* acc, V* jv,
-                                               const Src<V>& s) {
+  static constexpr bool kCustomDiag = true;  // the FP64 kernel calls diag<double>
+  template <class W>
+  __device__ __forceinline__ static void pair2(const Tgt<W>& t, W* acc, W* jv,
+                                               const Src<W>& s) {
+    using V = W;
     const V rx = t.x - s.x, ry = t.y - s.y, rz = t.z - s.z;
     V sg, s2;
     pair_core<UC>(t, s, sg, s2);
@@ -463,7 +476,6 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
     jv[7] = fma(h, ry, jv[7]);
     jv[8] = fma(h, rz, jv[8]);
     // vorticity filter sums: kernel values zeroed for r^2 <= 1e-8
-    const float eps = float(kRefEps);
     V ki, kj;
     if constexpr (UC) {
       ki = t.s4c * y7;
@@ -479,8 +491,8 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
       const V yj3 = yj2 * yj;
       kj = t.s4c * ((yj3 * yj3) * yj);
     }
-    ki = make_float2(r2.x > eps ? ki.x : 0.f, r2.y > eps ? ki.y : 0.f);
-    kj = make_float2(r2.x > eps ? kj.x : 0.f, r2.y > eps ? kj.y : 0.f);
+    ki = keep_if_gt(r2, kRefEps, ki);
+    kj = keep_if_gt(r2, kRefEps, kj);
     acc[9] = fma(ki, s.ax, acc[9]);
     acc[10] = fma(ki, s.ay, acc[10]);
     acc[11] = fma(ki, s.az, acc[11]);
@@ -494,15 +506,18 @@ struct OpLesStepBoth : RotStd<OpLesStep<float2, REFINE, UC>, UC> {
     acc[12] = fma(ke, fma(t.ax, s.ax, fma(t.ay, s.ay, t.az * s.az)), acc[12]);
   }
   // one-sided pair of the diagonal tiles: the one-sided operator's 15 sums, its enstrophy
-  // components E_i dotted with a_i into value 12
-  __device__ __forceinline__ static void diag(const Tgt<V>& t, V* acc, const Src<V>& s,
+  // components E_i dotted with a_i into value 12 (any lane type)
+  template <class W>
+  __device__ __forceinline__ static void diag(const Tgt<W>& t, W* acc, const Src<W>& s,
                                               const int64_t*, int64_t) {
-    V full[OneSided::NV];
-    static_assert(OneSided::NV == 15, "velocity, stretching, vorticity, 3 enstrophy sums");
+    using V = W;
+    using One = OpLesStep<W, REFINE, UC>;
+    V full[One::NV];
+    static_assert(One::NV == 15, "velocity, stretching, vorticity, 3 enstrophy sums");
 #pragma unroll
     for (int v = 0; v < 12; ++v) full[v] = acc[v];
-    full[12] = full[13] = full[14] = make_float2(0.f, 0.f);
-    OneSided::pair(t, full, s, nullptr, 0);
+    full[12] = full[13] = full[14] = splat<V>(0.0);
+    One::pair(t, full, s, nullptr, 0);
 #pragma unroll
     for (int v = 0; v < 12; ++v) acc[v] = full[v];
     acc[12] = fma(t.ax, full[12], fma(t.ay, full[13], fma(t.az, full[14], acc[12])));
@@ -930,7 +945,8 @@ rot_sweep_kernel(const RotArgs a) {
 
 // Both32: the FP32 both-sides operator whose pair2 (a template in the lane type) gives the
 // pair terms; OneSided64: the one-sided FP64 operator of the diagonal tiles.
-template <class Both32, class OneSided64, bool UC, int MINB = VPM_ROT64_MINB>
+template <class Both32, class OneSided64, bool UC, int MINB = VPM_ROT64_MINB,
+          int P = VPM_ROT64_P>
 struct OpBoth64 {
   using V = double;
   using Record = Rec<double>;
@@ -939,9 +955,10 @@ struct OpBoth64 {
   using SrcT = Src<double>;
   static constexpr bool kFP64 = true;
   static constexpr int NV = Both32::NV;
-  static constexpr int kP = VPM_ROT64_P;  // rot_tile: 64 kP warps = 32 R warps
+  static constexpr int kP = P;  // rot_tile: 64 kP warps = 32 R warps
   static constexpr int kMinBlocks = MINB;
-  static constexpr int kSymFrom = NV;
+  // values from kSymFrom on are taken once per unordered pair on the target side only
+  static constexpr int kSymFrom = Both32::kSymFrom;
   static constexpr bool kUniformCore = UC;
   __device__ __forceinline__ static SrcT load(const Record* rec, int64_t j, int64_t n) {
     if (j < n) return load_src<double>(rec[j]);
@@ -968,6 +985,12 @@ struct OpBoth64 {
                                                const SrcT& s) {
     Both32::pair2(t, acc, jv, s);
   }
+  __device__ __forceinline__ static void diag(const TgtT& t, double* acc, const SrcT& s) {
+    if constexpr (Both32::kCustomDiag)
+      Both32::diag(t, acc, s, nullptr, 0);
+    else
+      OneSided::pair(t, acc, s, nullptr, 0);
+  }
 };
 template <bool UC>
 using OpVelStretchBoth64 =
@@ -977,6 +1000,10 @@ template <bool UC>
 using OpVelBoth64 = OpBoth64<OpVelBoth<false, UC>, OpVel<double, false, UC>, UC, 3>;
 template <bool UC>
 using OpPseBoth64 = OpBoth64<OpPseBoth<false, UC>, OpPse<double, false, UC>, UC, 3>;
+// the LES step's 13 sums: two FP64 targets per lane (256-particle tiles)
+template <bool UC>
+using OpLesStepBoth64 =
+    OpBoth64<OpLesStepBoth<false, UC>, OpLesStep<double, false, UC>, UC, 2, 1>;
 
 template <class Op, bool DIAG>
 __global__ void __launch_bounds__(kRotThreads, Op::kMinBlocks)
@@ -987,8 +1014,9 @@ rot64_sweep_kernel(const RotArgs a) {
   constexpr int T = rot_tile<Op>();
   constexpr int WT = kRotWarps * 32;
   static_assert(T == R * WT, "a tile is the CTA's lanes times their targets");
+  constexpr int NJ = Op::kSymFrom;  // values with a source side: the first NJ
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  double* jbuf = reinterpret_cast<double*>(smem_raw);  // [NV][WT]
+  double* jbuf = reinterpret_cast<double*>(smem_raw);  // [NJ][WT]
   const Record* rec = static_cast<const Record*>(a.rec);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1030,7 +1058,7 @@ rot64_sweep_kernel(const RotArgs a) {
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         if constexpr (DIAG)
-          Op::OneSided::pair(tg[r], acc[r], cur, nullptr, 0);
+          Op::diag(tg[r], acc[r], cur);
         else
           Op::pair2(tg[r], acc[r], jv, cur);
       }
@@ -1038,16 +1066,16 @@ rot64_sweep_kernel(const RotArgs a) {
       Op::shuffle(cur, src_lane);
       if constexpr (!DIAG) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) jv[v] = __shfl_sync(0xffffffffu, jv[v], src_lane);
+        for (int v = 0; v < NJ; ++v) jv[v] = __shfl_sync(0xffffffffu, jv[v], src_lane);
       }
     }
     if constexpr (!DIAG) {
       // the warps' sums of source b * 32 + lane, added over the warps in a fixed order
 #pragma unroll
-      for (int v = 0; v < NV; ++v) jbuf[v * WT + warp * 32 + lane] = jv[v];
+      for (int v = 0; v < NJ; ++v) jbuf[v * WT + warp * 32 + lane] = jv[v];
       __syncthreads();
       const int nsrc = (cnt - b * 32 < 32) ? cnt - b * 32 : 32;
-      for (int q = tid; q < 32 * NV; q += kRotThreads) {
+      for (int q = tid; q < 32 * NJ; q += kRotThreads) {
         const int v = q >> 5, jj = q & 31;
         if (jj >= nsrc) continue;
         double sum = 0.0;
@@ -1063,8 +1091,12 @@ rot64_sweep_kernel(const RotArgs a) {
   for (int r = 0; r < R; ++r) {
     if (ti[r] < a.n) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v)
-        atomicAdd(&a.acc[(int64_t(set_i) * NV + v) * a.n + ti[r]], acc[r][v]);
+      for (int v = 0; v < NV; ++v) {
+        // a symmetric sum taken once per unordered pair elsewhere: the diagonal tiles visit
+        // every ordered pair, so they count half (the finalize doubles the sum)
+        const double w = (DIAG && v >= NJ) ? 0.5 * acc[r][v] : acc[r][v];
+        atomicAdd(&a.acc[(int64_t(set_i) * NV + v) * a.n + ti[r]], w);
+      }
     }
   }
 }

@@ -160,6 +160,41 @@ def test_fp64_both_sides_vs_oracle(uniform_core):
     assert kernels.device_errors() == 0
 
 
+@pytest.mark.parametrize("ring,uniform_core", [(False, False), (True, True)])
+def test_fp64_les_step_sums_both_sides_vs_one_sided(ring, uniform_core):
+    """The FP64 LES step sums at N >= 24576 take the both-sides schedule (13 sums: the
+    enstrophy filter sum once per unordered pair, target side only, the diagonal tiles at half
+    weight); they equal the one-sided FP64 sums up to rounding (1e-12)."""
+    from openonda_b200 import configs, kernels
+
+    if ring:
+        f = configs.les_ring(n_azimuthal=256, n_section=128)
+    else:
+        f = _field(30000, 31, False)
+    if uniform_core:
+        f.radii[:] = f.radii[0]
+    n = f.n
+    x, a, s = (torch.from_numpy(np.ascontiguousarray(z)).cuda()
+               for z in (f.positions, f.strengths, f.radii))
+    assert kernels.sweep_launches("les_step_sums", "fp64", n, n) > 2
+    both = kernels.les_step_sums(x, a, s, precision="fp64", uniform_core=uniform_core)
+    again = kernels.les_step_sums(x, a, s, precision="fp64", uniform_core=uniform_core)
+    prev = kernels.set_symmetric_min_n(1 << 40)
+    try:
+        one = kernels.les_step_sums(x, a, s, precision="fp64", uniform_core=uniform_core)
+    finally:
+        kernels.set_symmetric_min_n(prev)
+    for k, name in enumerate(("velocity", "stretching", "vorticity")):
+        e = normwise(both[k].cpu().numpy(), one[k].cpu().numpy())
+        print(f"ring={ring} uc={uniform_core} {name}: {e:.2e}")
+        assert e <= 1e-12, (name, e)
+        assert torch.equal(both[k], again[k])
+    ee = abs(float(both[3]) - float(one[3])) / abs(float(one[3]))
+    print(f"ring={ring} uc={uniform_core} enstrophy: {ee:.2e}")
+    assert ee <= 1e-12
+    assert kernels.device_errors() == 0
+
+
 def test_both_sides_is_deterministic(both_sides_always):
     from openonda_b200 import kernels
 
@@ -241,8 +276,8 @@ def test_velocity_and_pse_both_sides_vs_fp64(op, n, ring, uniform_core):
 
 def test_helicity_and_shards_stay_one_sided(both_sides_always):
     """Only whole-set self sums take the both-sides sweep: in FP32c the fused, velocity, PSE
-    and LES step sums and the adjoint, in FP64 the fused, velocity and PSE sums; the
-    diagnostics, the stretching-only sum and target shards (m < n) stay one-sided."""
+    and LES step sums and the adjoint, in FP64 the fused, velocity, PSE and LES step sums;
+    the diagnostics, the stretching-only sum and target shards (m < n) stay one-sided."""
     from openonda_b200 import kernels
 
     n = 4096
@@ -253,7 +288,7 @@ def test_helicity_and_shards_stay_one_sided(both_sides_always):
     for prec in ("fp32c", "fp64"):
         assert kernels.sweep_launches("strength_gradients", prec, n, n) == 2
     for op in ("velocity_and_strength_gradients", "selfinduced_velocity",
-               "strength_gradients_pse"):
+               "strength_gradients_pse", "les_step_sums"):
         assert kernels.sweep_launches(op, "fp64", n, n) > 2
         assert kernels.sweep_launches(op, "fp64", 1000, n) == 2
 
