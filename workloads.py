@@ -343,7 +343,10 @@ def config5(args):
 def sweeps(args):
     """Time of each FP32c sweep of an LES step on the dynamic-LES ring (default N = 2^20):
     the fused LES step sums against the separate sweeps they replace, plus PSE and the
-    velocity-only RK-stage sweep."""
+    velocity-only RK-stage sweep.  With --precision fp64: the FP64 self sums that take the
+    both-sides schedule, each also timed one-sided (general cores)."""
+    if args.precision == "fp64":
+        return _sweeps_fp64(args)
     n = args.n or (1 << 20)
     k = 1 << (int(np.log2(n)) // 2)
     f = configs.les_ring(n_azimuthal=k, n_section=n // k)
@@ -380,6 +383,41 @@ def sweeps(args):
             _emit({"sweep": name, "uniform_core": uc, "n": n, "precision": p,
                    "ms": round(ms, 2),
                    "gpairs_per_s": round(float(n) * n / (ms / 1e3) / 1e9, 1)})
+
+
+def _sweeps_fp64(args):
+    n = args.n or (1 << 20)
+    k = 1 << (int(np.log2(n)) // 2)
+    f = configs.les_ring(n_azimuthal=k, n_section=n // k)
+    n = f.n
+    r = lambda z: torch.from_numpy(np.asarray(z, np.float64)).cuda()
+    x, a, s, nu = r(f.positions), r(f.strengths), r(f.radii), r(f.viscosities)
+    p = "fp64"
+    cases = {
+        "les_step_sums": lambda: kernels.les_step_sums(x, a, s, precision=p),
+        "velocity_and_strength_gradients":
+            lambda: kernels.velocity_and_strength_gradients(x, a, s, precision=p),
+        "strength_gradients_pse": lambda: kernels.strength_gradients_pse(x, a, s, nu,
+                                                                         precision=p),
+        "selfinduced_velocity": lambda: kernels.selfinduced_velocity(x, a, s, precision=p),
+    }
+    reps = args.steps or 1
+    for name, fn in cases.items():
+        row = {"sweep": name, "n": n, "precision": p}
+        for sched, thr in (("both_sides", None), ("one_sided", 1 << 40)):
+            old = kernels.set_symmetric_min_n(thr) if thr is not None else None
+            try:
+                fn()
+                with _Timer() as t:
+                    for _ in range(reps):
+                        fn()
+            finally:
+                if old is not None:
+                    kernels.set_symmetric_min_n(old)
+            ms = t.ms / reps
+            row[sched] = {"ms": round(ms, 1),
+                          "gpairs_per_s": round(float(n) * n / (ms / 1e3) / 1e9, 1)}
+        _emit(row)
 
 
 def pairshards(args):
@@ -632,6 +670,7 @@ def main():
     ap.add_argument("--fd", type=int, default=None)
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--sizes", type=int, nargs="*", default=None)
+    ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
     args = ap.parse_args()
     globals()[args.workload](args)
 
