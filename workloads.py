@@ -344,7 +344,7 @@ def sweeps(args):
     """Time of each FP32c sweep of an LES step on the dynamic-LES ring (default N = 2^20):
     the fused LES step sums against the separate sweeps they replace, plus PSE and the
     velocity-only RK-stage sweep.  With --precision fp64: the FP64 self sums that take the
-    both-sides schedule, each also timed one-sided (general cores)."""
+    both-sides schedule, each also timed one-sided (general cores, or --uniform-core)."""
     if args.precision == "fp64":
         return _sweeps_fp64(args)
     n = args.n or (1 << 20)
@@ -393,17 +393,21 @@ def _sweeps_fp64(args):
     r = lambda z: torch.from_numpy(np.asarray(z, np.float64)).cuda()
     x, a, s, nu = r(f.positions), r(f.strengths), r(f.radii), r(f.viscosities)
     p = "fp64"
+    uc = bool(args.uniform_core)  # the ring has one core
     cases = {
-        "les_step_sums": lambda: kernels.les_step_sums(x, a, s, precision=p),
+        "les_step_sums": lambda: kernels.les_step_sums(x, a, s, precision=p, uniform_core=uc),
         "velocity_and_strength_gradients":
-            lambda: kernels.velocity_and_strength_gradients(x, a, s, precision=p),
+            lambda: kernels.velocity_and_strength_gradients(x, a, s, precision=p,
+                                                            uniform_core=uc),
         "strength_gradients_pse": lambda: kernels.strength_gradients_pse(x, a, s, nu,
-                                                                         precision=p),
-        "selfinduced_velocity": lambda: kernels.selfinduced_velocity(x, a, s, precision=p),
+                                                                         precision=p,
+                                                                         uniform_core=uc),
+        "selfinduced_velocity": lambda: kernels.selfinduced_velocity(x, a, s, precision=p,
+                                                                     uniform_core=uc),
     }
     reps = args.steps or 1
     for name, fn in cases.items():
-        row = {"sweep": name, "n": n, "precision": p}
+        row = {"sweep": name, "n": n, "precision": p, "uniform_core": uc}
         for sched, thr in (("both_sides", None), ("one_sided", 1 << 40)):
             old = kernels.set_symmetric_min_n(thr) if thr is not None else None
             try:
@@ -671,6 +675,7 @@ def main():
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--sizes", type=int, nargs="*", default=None)
     ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
+    ap.add_argument("--uniform-core", action="store_true")
     args = ap.parse_args()
     globals()[args.workload](args)
 
