@@ -173,30 +173,28 @@ class ShardedVelocityStretching:
         # records as float rows so the collective moves whole records
         words = self.rec_bytes // 4
         self.local = torch.empty((self.m, words), dtype=torch.float32, device=dev)
-        self.ws_bytes = kernels.workspace_bytes("velocity_and_strength_gradients", precision,
-                                                self.m, self.n)
-        self.ws = torch.empty(max(self.ws_bytes, 256), dtype=torch.uint8, device=dev)
         self.u = torch.empty((self.m, 3), dtype=torch.float64, device=dev)
         self.g = torch.empty((self.m, 3), dtype=torch.float64, device=dev)
-        # pack, then the sweep's own launches (one-sided: sweep + finalize; both-sides sweep
-        # over all particles: zero, diagonal tiles, diagonal-pair launches, finalize)
-        self.sweep_launches = int(lib.vpm_sweep_launches(
-            _lib.OPS["velocity_and_strength_gradients"], self.pcode, self.m, self.n))
-        self.both_sides = self.sweep_launches > 2
-        self.kernel_launches_per_call = 1 + self.sweep_launches
         # pair shards: several ranks and a size that takes the both-sides schedule
-        self.pairs = None
-        if self.world > 1:
-            self.pairs = self._pair_plan(lib)
+        self.pairs = self._pair_plan(lib) if self.world > 1 else None
         if self.pairs is not None:
             nt, npairs, per_launch, nv, wsb, (t0, t1, p0, p1) = self.pairs
             self.both_sides = True
-            self.ws = torch.empty(max(wsb, 256), dtype=torch.uint8, device=dev)
+            self.ws_bytes = wsb
             self.rows = torch.empty((self.n, nv), dtype=torch.float64, device=dev)
             launches = -(-(p1 - p0) // per_launch)
             # zero, diagonal tiles, diagonal-pair launches, rows, finalize (+ pack)
             self.sweep_launches = 1 + (1 if t1 > t0 else 0) + launches + 2
-            self.kernel_launches_per_call = 1 + self.sweep_launches
+        else:
+            self.ws_bytes = kernels.workspace_bytes("velocity_and_strength_gradients",
+                                                    precision, self.m, self.n)
+            # the sweep's own launches (one-sided: sweep + finalize; both-sides sweep over all
+            # particles: zero, diagonal tiles, diagonal-pair launches, finalize)
+            self.sweep_launches = int(lib.vpm_sweep_launches(
+                _lib.OPS["velocity_and_strength_gradients"], self.pcode, self.m, self.n))
+            self.both_sides = self.sweep_launches > 2
+        self.ws = torch.empty(max(self.ws_bytes, 256), dtype=torch.uint8, device=dev)
+        self.kernel_launches_per_call = 1 + self.sweep_launches  # + the pack
 
     def _pair_plan(self, lib):
         layout = pairs_layout(self.n, self.precision)
